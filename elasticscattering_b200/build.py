@@ -1,0 +1,129 @@
+"""Builds the in-tree native libraries of elasticscattering_b200.
+
+    libes_cuda.so   CUDA kernels for sm_100a + the C ABI of include/es_cuda.h
+    libes_host.so   host C++ runtime (Grid, config parser, runner, logger,
+                    SimulationCUDA) over the C ABI
+    es_b200         the command-line driver (drop-in for the reference's CLI)
+
+Plain nvcc/g++ invocations, rebuilt only when a source is newer than its
+output. Used by __graft_entry__.build() and by `python -m elasticscattering_b200.build`.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+HOST = PKG / "host"
+INCLUDE = ROOT / "include"
+OBJ = PKG / "_build"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_COMMON = ARCH + [
+    "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+    f"-I{INCLUDE}", f"-I{CSRC}",
+]
+# Per-translation-unit device flags. The plain FP64 path keeps the reference's
+# rounding: no multiply-add contraction (IEEE div/sqrt are nvcc's default).
+CUDA_UNITS = {
+    "es_context.cu": ["-fmad=false"],
+    "es_lifetime_fp64.cu": ["-fmad=false"],
+    "es_integrate.cu": ["-fmad=false"],
+    "es_probe.cu": [],
+}
+
+HOST_UNITS = ["grid.cpp", "config.cpp", "logger.cpp", "simulation_cuda.cpp", "runner.cpp"]
+GXX_COMMON = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
+              f"-I{INCLUDE}", f"-I{HOST}"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(out: Path, deps: list[Path]) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(d.exists() and d.stat().st_mtime > t for d in deps)
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {cmd[0]} ... {cmd[-1]}")
+
+
+def _headers(d: Path) -> list[Path]:
+    return sorted(list(d.glob("*.h")) + list(d.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
+
+
+def build_cuda(verbose_ptxas: bool = False) -> Path:
+    OBJ.mkdir(exist_ok=True)
+    out = PKG / "libes_cuda.so"
+    hdrs = _headers(CSRC)
+    objs = []
+    jobs = []
+    for unit, flags in CUDA_UNITS.items():
+        src = CSRC / unit
+        obj = OBJ / (unit + ".o")
+        objs.append(obj)
+        if verbose_ptxas or _stale(obj, [src] + hdrs):
+            cmd = [nvcc()] + NVCC_COMMON + flags + ["-c", str(src), "-o", str(obj)]
+            if verbose_ptxas:
+                cmd += ["-Xptxas", "-v"]
+            jobs.append(cmd)
+    with ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        list(ex.map(_run, jobs))
+    if jobs or _stale(out, objs):
+        _run([nvcc()] + ARCH + ["-shared", "-o", str(out)] + [str(o) for o in objs])
+    return out
+
+
+def build_host() -> list[Path]:
+    """Host C++ runtime: libes_host.so (+ the es_b200 CLI once main.cpp exists)."""
+    srcs = [HOST / u for u in HOST_UNITS if (HOST / u).exists()]
+    if not srcs:
+        return []
+    OBJ.mkdir(exist_ok=True)
+    lib = PKG / "libes_host.so"
+    hdrs = _headers(HOST)
+    if _stale(lib, srcs + hdrs + [PKG / "libes_cuda.so"]):
+        _run(["g++"] + GXX_COMMON + ["-shared", "-o", str(lib)] + [str(s) for s in srcs]
+             + [f"-L{PKG}", "-les_cuda", "-Wl,-rpath,$ORIGIN"])
+    out = [lib]
+    main = HOST / "main.cpp"
+    cli = PKG / "es_b200"
+    if main.exists():
+        if _stale(cli, [main, lib] + hdrs):
+            _run(["g++"] + GXX_COMMON + ["-o", str(cli), str(main), f"-L{PKG}", "-les_host", "-les_cuda",
+                                          "-Wl,-rpath,$ORIGIN"])
+        out.append(cli)
+    return out
+
+
+def build_oracle() -> None:
+    """Test checkers: oracle/liboracle.so, and oracle/_ref when the reference tree exists."""
+    _run(["make", "-s", "-C", str(ROOT / "oracle")])
+
+
+def build_all(verbose_ptxas: bool = False) -> None:
+    build_cuda(verbose_ptxas)
+    build_host()
+    build_oracle()
+
+
+if __name__ == "__main__":
+    build_all(verbose_ptxas="-v" in sys.argv)
+    print("built", PKG / "libes_cuda.so")

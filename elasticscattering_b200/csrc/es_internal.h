@@ -1,0 +1,92 @@
+// es_internal.h - launch interfaces shared by the translation units of
+// libes_cuda.so. Not part of the public ABI (include/es_cuda.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace es {
+
+// Device-side metric slots (es_metrics order).
+enum MetricSlot : int {
+    kMetCells = 0,
+    kMetImps = 1,
+    kMetInside = 2,
+    kMetEscaped = 3,
+    kMetAtBound = 4,
+    kMetMaxImps = 5,
+    kMetMaxCells = 6,
+    kMetCrossings = 7,
+    kMetStartTests = 8,
+    kMetCount = 9
+};
+
+// Device error bits (written with atomicOr, read by es_synchronize).
+enum DeviceError : int { kErrWalkCap = 1, kErrStartCell = 2 };
+
+// Per-phase constants of one sector, tabulated on the host by es_init_sample
+// with the reference's expressions (CreateParticle, src/sim/es/lifetime.h:36-58):
+// phi, velocity (cos(phi) * v, sin(phi) * v) from the host libm, and the
+// angle to the sector bound (GetBoundTime's dphi, src/sim/es/details.h:219-228;
+// unused for the coherent sector, whose bound time is INF). The field-dependent parts
+// (orbit-centre shift, bound time = dphi / w) are finished in the kernel with
+// the same IEEE operations.
+struct PhaseOrbit {
+    double phi, vel_x, vel_y, bound_dphi;
+};
+
+// Per-phase integration constants (ApplySigma, src/sim/SimulationCPU.cpp:186-192):
+// phi, cos(phi), sin(phi) (host libm) and the phase Simpson weight.
+struct PhaseSigma {
+    double phi, cos_phi, sin_phi, weight;
+};
+
+struct LifetimeLaunch {
+    const double2* imps;
+    const int* cell_end;
+    const PhaseOrbit* phase;
+    double* out;                  // n_orbits raw lifetimes, [j][i][q][p]
+    float* out32;                 // optional FP32 copy (split path), may be null
+    unsigned long long* metrics;  // kMetCount slots
+    int* error;
+    double spawn_start, spawn_size, cell_size, imp_radius;
+    double speed, radius, radius_sq, w, dist, off_x, off_y;
+    long long n_orbits;
+    int cpr, dim, n_phase, clockwise, coherent, walk_cap;
+    int row0;                     // first start-position row of this launch
+};
+
+constexpr int kIntegrateBlocks = 296;   // 2 x 148 SMs; fixed so the reduction order is fixed
+constexpr int kIntegrateThreads = 256;
+constexpr int kMaxTChunk = 8;           // temperatures integrated per pass over the lifetimes
+
+// One group of up to kMaxTChunk temperatures; all per-temperature constants
+// travel by value in the launch, so no device parameter buffers are needed.
+struct IntegrateLaunch {
+    const double* lifetimes;      // raw lifetimes, [pos][phase]
+    const PhaseSigma* phase;
+    double tau[kMaxTChunk];       // GetTau per temperature
+    double max_lt[kMaxTChunk];    // GetDefaultMaxLifetime = 15 * tau
+    double factor[kMaxTChunk];    // GetSigmaIntegrandFactor
+    double* pos_lt;               // optional per-position maps [t][pos] (images), may be null
+    double* pos_xx;
+    double* pos_xy;
+    double* partial;              // [t][block][2] block partial sums (xx, xy), scratch
+    double* sigma_out;            // [t][2] for this group
+    double w_signed;
+    double phi_integrand_factor;
+    int dim, n_phase, n_t;        // n_t <= kMaxTChunk
+    int n_blocks;                 // partial blocks per temperature
+};
+
+cudaError_t launch_lifetimes_fp64(const LifetimeLaunch& L, cudaStream_t s);
+// Stages (b)+(c) for one temperature group: two launches.
+cudaError_t launch_integrate(const IntegrateLaunch& L, cudaStream_t s);
+cudaError_t launch_debug_trace(const LifetimeLaunch& L, const PhaseOrbit& ph, double px, double py, double* d_out,
+                               cudaStream_t s);
+cudaError_t launch_debug_next_cell(double cx, double cy, double r, int clockwise, double phi, double start,
+                                   double size, double cell, int cpr, const double* d_in6, double* d_out6,
+                                   int* d_avail, cudaStream_t s);
+
+}  // namespace es

@@ -1,0 +1,106 @@
+"""Named workloads of the conductivity path, as concrete reference inputs.
+
+Each workload is a set of reference `.config` values (src/SimulationConfiguration.h)
+plus the field and temperature lists of its sweep. Conventions used to turn
+the physical descriptions into reference inputs:
+
+- phase samples N_phi -> phi_steps = the odd integer nearest N_phi/4 (the
+  reference integrates each quarter separately, src/sim/Simulation.h:115-125);
+- "padded by one orbit diameter" -> region_extends = 2 v m* / (e B_min);
+- "cell size ~5e-8 m" -> the integer target_cell_population whose
+  cells_per_row = round(sqrt(N_imp / tcp)) gives the nearest cell size;
+- seed s -> start_seed s, so sample k uses Grid seed (s + 100) * (k + 1)
+  (src/SimulationConfiguration.h:209-210);
+- T = 0 cannot be expressed by the reference (its parser drops T <= 0,
+  src/SimulationConfiguration.h:193-195, and tau_inc = hbar / (k_B T) diverges).
+  The "T = 0" row is the coherent sigma at the configured tau plus the
+  incoherent sigma at T_ZERO_STANDIN kelvin.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+# src/sim/es/constants.h:23-26
+M0 = 9.10938188e-31
+M_EFF = 5.0 * M0
+E_CHARGE = 1.60217646e-19
+
+T_ZERO_STANDIN = 1e-3  # kelvin
+
+
+def orbit_diameter(speed: float, b_min: float) -> float:
+    """2 r = 2 v m* / (e B) at the smallest field of the sweep."""
+    return 2.0 * speed * M_EFF / (E_CHARGE * b_min)
+
+
+@dataclass
+class Workload:
+    name: str
+    dim: int                 # `dimension`: start positions per row (odd)
+    phi_steps: int           # `phi_steps`: phases per quadrant (odd)
+    region_size: float
+    region_extends: float
+    density: float
+    impurity_radius: float
+    target_cell_population: int
+    fields: list = field(default_factory=list)
+    temperatures: list = field(default_factory=list)
+    start_seed: int = 0
+    num_samples: int = 1
+    particle_speed: float = 1.68e5
+    alpha: float = 0.3
+    tau: float = 1e-12
+    clockwise: bool = True
+
+    @property
+    def orbits_per_pass(self) -> int:
+        return self.dim * self.dim * 4 * self.phi_steps
+
+    def seed(self, sample: int) -> int:
+        return (self.start_seed + 100) * (sample + 1)
+
+    def config_text(self) -> str:
+        """The workload as a reference .config file."""
+        temps = " ".join(repr(float(t)) for t in self.temperatures)
+        lines = [
+            f"num_samples {self.num_samples}", f"dimension {self.dim}", f"phi_steps {self.phi_steps}",
+            f"temperatures {temps}",
+        ]
+        if len(self.fields) == 1:
+            lines.append(f"magnetic_field {self.fields[0]!r}")
+        else:
+            lo, hi = self.fields[0], self.fields[-1]
+            lines += [f"magnetic_field_min {lo!r}", f"magnetic_field_max {hi!r}", f"magnetic_field_n {len(self.fields)}"]
+        lines += [
+            f"particle_speed {self.particle_speed!r}", f"clockwise {1 if self.clockwise else 0}",
+            f"alpha {self.alpha!r}", f"tau {self.tau!r}", f"region_size {self.region_size!r}",
+            f"region_extends {self.region_extends!r}", f"impurity_density {self.density!r}",
+            f"impurity_radius {self.impurity_radius!r}", f"target_cell_population {self.target_cell_population}",
+            f"start_seed {self.start_seed}",
+        ]
+        return "\n".join(lines) + "\n"
+
+
+def config0() -> Workload:
+    """Plain method, CPU-runnable: 65x65 positions x 101 phase samples, 1e15 m^-2, B = 20 T."""
+    return Workload("config0-65x65x100-B20", dim=65, phi_steps=25, region_size=1e-6,
+                    region_extends=orbit_diameter(1.68e5, 20.0), density=1e15, impurity_radius=2e-9,
+                    target_cell_population=3, fields=[20.0], temperatures=[T_ZERO_STANDIN])
+
+
+def config1() -> Workload:
+    """Plain method at scale: 257x257 positions x 513 phase samples (34.08 M orbits per
+    sector pass), 5e15 m^-2, B in {1, 5, 10, 20, 40} T, one sample."""
+    return Workload("config1-257x257x516-5B", dim=257, phi_steps=129, region_size=1e-6,
+                    region_extends=orbit_diameter(1.68e5, 1.0), density=5e15, impurity_radius=2e-9,
+                    target_cell_population=12, fields=[1.0, 5.0, 10.0, 20.0, 40.0], temperatures=[T_ZERO_STANDIN])
+
+
+def config3() -> Workload:
+    """Precision stress: 1025x1025 positions x 1025 phases, 1e16 m^-2, r_i = 5e-9, B = 40 T."""
+    return Workload("config3-1025x1025x1028-B40", dim=1025, phi_steps=257, region_size=1e-6,
+                    region_extends=orbit_diameter(1.68e5, 40.0), density=1e16, impurity_radius=5e-9,
+                    target_cell_population=25, fields=[40.0], temperatures=[T_ZERO_STANDIN])
+
+
+WORKLOADS = {"config0": config0, "config1": config1, "config3": config3}

@@ -1,0 +1,206 @@
+/* es_cuda.h - C ABI of the B200 (sm_100a) backend for ElasticScattering's
+ * real-space conductivity path.
+ *
+ * The reference selects a backend behind `class Simulation`
+ * (src/sim/Simulation.h:56-147; chosen at src/SimulationRunner.cpp:82-84) and
+ * its GPU implementation is an OpenCL context with six kernels
+ * (src/sim/SimulationCL.cpp, src/sim/cl/*.cl). This header is the drop-in
+ * replacement for that implementation: plain pointers and sizes, no C++ or
+ * framework types. A host wrapper (SimulationCUDA, elasticscattering_b200/host)
+ * maps the reference's `Simulation` methods onto these calls one to one.
+ *
+ * Conventions
+ *  - Every call returns es_status; ES_OK == 0. After a failure, es_last_error()
+ *    returns a message. The reference prints and exit(0)s instead
+ *    (src/utils/ErrorMacros.h:22-38); the host wrapper restores that behaviour.
+ *  - One context = one device + one CUDA stream. Calls on a context are
+ *    serialised on its stream; distinct contexts share no state.
+ *  - Host arrays are caller-owned. The context owns its device buffers.
+ *  - Orbit order is the reference's [j][i][q][p]: index
+ *    j*dim*4*ppq + i*4*ppq + q*ppq + p (src/sim/Simulation.h:67).
+ */
+#ifndef ES_CUDA_H
+#define ES_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum es_status {
+    ES_OK = 0,
+    ES_ERR_BAD_ARG = 1,     /* invalid size, pointer or state */
+    ES_ERR_OOM = 2,         /* device allocation failed */
+    ES_ERR_LAUNCH = 3,      /* kernel launch or CUDA API failure */
+    ES_ERR_WALK_CAP = 4,    /* an orbit exceeded the cell-walk step bound */
+    ES_ERR_DEVICE = 5,      /* no usable CUDA device / wrong architecture */
+    ES_ERR_NO_GRID = 6,     /* es_upload_grid has not been called */
+    ES_ERR_NO_SAMPLE = 7,   /* es_init_sample has not been called */
+    ES_ERR_TIMEOUT = 8      /* a bounded device wait ran out */
+} es_status;
+
+typedef enum es_precision {
+    ES_PRECISION_FP64 = 0,  /* plain FP64, reference semantics operation by operation */
+    ES_PRECISION_SPLIT = 1  /* FP32 orbit stepping, FP64 tangency band, phase and reductions */
+} es_precision;
+
+/* Reference layout of ImpuritySettings (src/sim/es/settings.h:76-85). */
+typedef struct es_impurity_settings {
+    double spawn_region_start;
+    double spawn_region_size;
+    double cell_size;
+    int32_t cells_per_row;
+    double impurity_radius;
+} es_impurity_settings;
+
+/* The reference's Settings (src/ConfigSettings.h:22-34) with the bool widened
+ * to int32 for a stable C layout. */
+typedef struct es_settings {
+    double tau;
+    double alpha;
+    int32_t is_clockwise;
+    double particle_speed;
+    double region_size;
+    double region_extends;
+    double impurity_density;
+    double impurity_radius;
+    int32_t target_cell_population;
+} es_settings;
+
+/* ParticleMetrics (src/sim/es/particle_metrics.h:22-44) with 64-bit counters
+ * (the reference's int32 counters overflow beyond ~2^31 impurity tests). */
+typedef struct es_metrics {
+    int64_t cells_passed;
+    int64_t impurities_tested;
+    int64_t particles_inside_impurity;
+    int64_t particles_escaped;
+    int64_t particles_at_bound;
+    int64_t max_impurities_tested;
+    int64_t max_cells_passed;
+    int64_t crossings_tested; /* orbit/impurity pairs that passed CirclesCross (FLOP model) */
+    int64_t start_cell_tests; /* InsideImpurity tests of the start-cell scans (FLOP model) */
+} es_metrics;
+
+/* Constructor arguments of Simulation (src/sim/Simulation.h:131-146) plus
+ * the GridInformation it reads (src/sim/es/settings.h:65-73). */
+typedef struct es_sim_desc {
+    int32_t positions_per_row;      /* dim, odd, >= 3 */
+    int32_t particles_per_quadrant; /* phi_steps, odd, >= 3 */
+    double region_size;
+    double region_extends;
+    double grid_cell_size;          /* GridInformation::cell_size (sets the start offset) */
+    int32_t device_ordinal;
+    int32_t precision;              /* es_precision */
+} es_sim_desc;
+
+typedef struct es_ctx es_ctx;
+
+/* Replaces SimulationCL::SimulationCL (src/sim/SimulationCL.cpp:386-475): binds a
+ * device, creates the stream and the per-pass buffers. */
+es_status es_create(const es_sim_desc* desc, es_ctx** out);
+
+/* Replaces SimulationCL::~SimulationCL (src/sim/SimulationCL.cpp:477-508). */
+es_status es_destroy(es_ctx* ctx);
+
+/* Message of the last failure on this context ("" if none). ctx may be NULL
+ * for failures of es_create. */
+const char* es_last_error(const es_ctx* ctx);
+
+/* Replaces the impurity/index upload in SimulationCL::ComputeLifetimes
+ * (src/sim/SimulationCL.cpp:119-125). imp_xy holds n_indexed ordered
+ * impurities as x,y pairs (Grid::GetImpurities, src/sim/Grid.h:74), cell_end
+ * the cumulative end index of each of cells_per_row^2 cells (Grid::GetIndex,
+ * src/sim/Grid.h:75). The upload is skipped when `generation` equals the
+ * generation already resident (the reference keys on the seed, which is 0 for
+ * every file-loaded grid). */
+es_status es_upload_grid(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
+                         const es_impurity_settings* is, uint64_t generation);
+
+/* Replaces Simulation::InitSample (src/sim/Simulation.h:111-126): sector
+ * (coherent or incoherent) and carrier settings for the following passes. */
+es_status es_init_sample(es_ctx* ctx, const es_settings* s, int32_t coherent);
+
+/* Replaces Simulation::ComputeSigmas (src/sim/Simulation.h:128,
+ * src/sim/SimulationCL.cpp:72-91): lifetimes of all orbits for field B
+ * (stage a), then per temperature the phase Simpson integral (stage b) and the
+ * start-position Simpson reduction (stage c). out_sigma receives
+ * [xx_0, xy_0, xx_1, xy_1, ...] (2*n_t doubles). out_metrics may be NULL.
+ * Blocks until the results are on the host. */
+es_status es_compute_sigmas(es_ctx* ctx, double magnetic_field, const double* temperatures, int32_t n_t,
+                            double* out_sigma, es_metrics* out_metrics);
+
+/* Replaces Simulation::ComputeSigmasWithImages (src/sim/Simulation.h:129,
+ * src/sim/SimulationCL.cpp:93-111): as es_compute_sigmas plus the per-position
+ * maps of IntegratePosition (src/sim/SimulationCPU.cpp:224-243): truncated
+ * lifetime, sigma_xx and sigma_xy integrated over phase, each dim*dim doubles
+ * per temperature, temperature-major. */
+es_status es_compute_sigmas_images(es_ctx* ctx, double magnetic_field, const double* temperatures, int32_t n_t,
+                                   double* out_sigma, double* lifetime_pos, double* sigma_xx_pos,
+                                   double* sigma_xy_pos, es_metrics* out_metrics);
+
+/* Replaces SimulationCL::ComputeLifetimes (src/sim/SimulationCL.cpp:113-177):
+ * stage (a) only. If out_lifetimes is non-NULL the dim^2*4*ppq raw lifetimes
+ * are copied to it (the `dump_lifetimes` option of the reference's config,
+ * examples/explanation.config:89-90). The lifetimes stay resident for
+ * es_derive_temperatures. */
+es_status es_compute_lifetimes(es_ctx* ctx, double magnetic_field, double* out_lifetimes, es_metrics* out_metrics);
+
+/* Replaces the temperature loop of SimulationCL::ComputeSigmas
+ * (src/sim/SimulationCL.cpp:82-84, DeriveTemperature :179-189) on the
+ * lifetimes resident from the last es_compute_lifetimes. */
+es_status es_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_t n_t, double* out_sigma);
+
+/* Asynchronous form of es_compute_sigmas for callers that keep results on the
+ * device: enqueues stages (a)-(c) on the context stream and writes 2*n_t
+ * doubles to the DEVICE pointer d_out_sigma. Metrics accumulate on the device
+ * until es_read_metrics. No host synchronisation. */
+es_status es_enqueue_sigmas(es_ctx* ctx, double magnetic_field, const double* temperatures, int32_t n_t,
+                            double* d_out_sigma);
+
+/* Asynchronous stage (a) only: enqueues the lifetime pass for field B on the
+ * context stream (SimulationCL::ComputeLifetimes without its blocking copies,
+ * src/sim/SimulationCL.cpp:113-177). The lifetimes stay resident. */
+es_status es_enqueue_lifetimes(es_ctx* ctx, double magnetic_field);
+
+/* Waits for the context stream, then reports any device-side error flag. */
+es_status es_synchronize(es_ctx* ctx);
+
+/* Reads (and optionally resets) the device-side metrics accumulated by
+ * es_enqueue_sigmas. Synchronises the stream. */
+es_status es_read_metrics(es_ctx* ctx, es_metrics* out, int32_t reset);
+
+/* The context's cudaStream_t, as an opaque pointer (for event timing). */
+void* es_stream(es_ctx* ctx);
+
+/* Number of kernel launches this context has issued since creation. */
+int64_t es_launch_count(const es_ctx* ctx);
+
+/* Known-answer hook for the device geometry: one GetNextCell step
+ * (src/sim/es/cell_grid.h:132-181) evaluated by the FP64 device code on one
+ * thread. in6/out6 = (pos.x, pos.y, incident_angle, dphi, cell.x, cell.y).
+ * Returns the step's "next cell available" flag in *out_available. */
+es_status es_debug_next_cell(es_ctx* ctx, double center_x, double center_y, double radius, int32_t clockwise,
+                             double phi, const es_impurity_settings* is, const double* in6, double* out6,
+                             int32_t* out_available);
+
+/* Known-answer hook for one orbit: CreateParticle(q, p, (px, py), ps) +
+ * TraceOrbit (src/sim/es/lifetime.h:36-148) on the resident grid, evaluated by
+ * the FP64 device code on one thread, with explicit ParticleSettings fields
+ * (src/sim/es/settings.h:87-98) as the reference's LifetimeTests build them.
+ * Writes the raw lifetime (seconds) to *out_lifetime. */
+es_status es_debug_trace(es_ctx* ctx, double px, double py, int32_t q, int32_t p, double magnetic_field,
+                         double phi_start, double phi_step_size, double alpha, double particle_speed,
+                         int32_t is_clockwise, int32_t is_coherent, double* out_lifetime);
+
+/* Measured FP64 FMA throughput of a device (TFLOP/s, 2 FLOP per FMA): the
+ * denominator of the lifetime kernel's roofline. No reference counterpart
+ * (the reference publishes no device figures). Runs for a few milliseconds. */
+es_status es_probe_fp64_fma(int32_t device_ordinal, double* out_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ES_CUDA_H */

@@ -390,6 +390,25 @@ double orc_trace_one(const orc_sim* s, const orc_impurity_settings* is, const do
     return trace(s, is, (const v2*)imp_xy, cell_end, w, pos, q, p, phi_start, phi_step, m, &c);
 }
 
+double orc_trace_explicit(const orc_impurity_settings* is, const double* imp_xy, const int32_t* cell_end,
+                          double magnetic_field, double px, double py, int32_t q, int32_t p, double phi_start,
+                          double phi_step, double alpha, double particle_speed, int32_t is_clockwise,
+                          int32_t is_coherent)
+{
+    orc_sim s;
+    memset(&s, 0, sizeof(s));
+    s.particle_speed = particle_speed;
+    s.alpha = alpha;
+    s.is_clockwise = is_clockwise;
+    s.is_coherent = is_coherent;
+    const double w = ES_E * magnetic_field / ES_M;
+    orc_metrics m;
+    memset(&m, 0, sizeof(m));
+    orbit_counts c = {0, 0};
+    const v2 pos = {px, py};
+    return trace(&s, is, (const v2*)imp_xy, cell_end, w, pos, q, p, phi_start, phi_step, &m, &c);
+}
+
 /* ---- src/sim/es/util.h and the integration in SimulationCPU.cpp --------- */
 
 /* SimpsonWeight, util.h:24-28 */

@@ -86,6 +86,13 @@ double orc_trace_one(const orc_sim* s, const orc_impurity_settings* is, const do
                      const int32_t* cell_end, double magnetic_field, double px, double py, int32_t q,
                      int32_t p, orc_metrics* m);
 
+/* One orbit with explicit ParticleSettings fields (src/sim/es/settings.h:87-98),
+ * as the reference's LifetimeTests build them (tests/es/LifetimeTests.h:19-34). */
+double orc_trace_explicit(const orc_impurity_settings* is, const double* imp_xy, const int32_t* cell_end,
+                          double magnetic_field, double px, double py, int32_t q, int32_t p, double phi_start,
+                          double phi_step, double alpha, double particle_speed, int32_t is_clockwise,
+                          int32_t is_coherent);
+
 /* ---- stages (b),(c): integration ---------------------------------------- */
 
 /* SimulationCPU::DeriveTemperature (src/sim/SimulationCPU.cpp:143-155): sigma xx, xy
