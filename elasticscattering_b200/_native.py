@@ -55,6 +55,11 @@ class Metrics(C.Structure):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
 
 
+class Tuning(C.Structure):
+    """es_tuning: kernel choices of a context."""
+    _fields_ = [("lifetime_variant", C.c_int32)]
+
+
 class SimDesc(C.Structure):
     _fields_ = [("positions_per_row", C.c_int32), ("particles_per_quadrant", C.c_int32),
                 ("region_size", C.c_double), ("region_extends", C.c_double), ("grid_cell_size", C.c_double),
@@ -66,6 +71,8 @@ _vp, _d, _i32, _i64, _u32, _u64 = C.c_void_p, C.c_double, C.c_int32, C.c_int64, 
 CUDA_API = {
     "es_create": (_i32, [C.POINTER(SimDesc), C.POINTER(_vp)]),
     "es_destroy": (_i32, [_vp]),
+    "es_get_tuning": (_i32, [_vp, C.POINTER(Tuning)]),
+    "es_set_tuning": (_i32, [_vp, C.POINTER(Tuning)]),
     "es_last_error": (C.c_char_p, [_vp]),
     "es_upload_grid": (_i32, [_vp, _vp, _i64, _vp, C.POINTER(ImpuritySettings), _u64]),
     "es_init_sample": (_i32, [_vp, C.POINTER(Settings), _i32]),

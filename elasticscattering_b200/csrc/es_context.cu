@@ -82,6 +82,8 @@ struct es_ctx {
     double* d_pos = nullptr;          // images: 3 * pos_cap doubles
     int64_t pos_cap = 0;
     double last_w = 0;                // angular speed of the resident lifetimes
+    unsigned long long* d_work = nullptr;  // orbit counter of the refill kernel
+    es_tuning tuning{es::kLifetimePerThreadLean};
     bool lifetimes_valid = false;
 };
 
@@ -177,6 +179,8 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.coherent = coherent;
     L.walk_cap = walk_cap_for(L.radius, L.cell_size);
     L.row0 = 0;
+    L.variant = ctx->tuning.lifetime_variant;
+    L.work = ctx->d_work;
     return L;
 }
 
@@ -294,6 +298,7 @@ void release(es_ctx* ctx)
     cudaFree(ctx->d_partial);
     cudaFree(ctx->d_sigma);
     cudaFree(ctx->d_pos);
+    cudaFree(ctx->d_work);
     if (ctx->h_sigma) cudaFreeHost(ctx->h_sigma);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -348,6 +353,7 @@ es_status es_create(const es_sim_desc* desc, es_ctx** out)
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_phase_sigma, sizeof(es::PhaseSigma) * n_phase);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_metrics, sizeof(unsigned long long) * es::kMetCount);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_work, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_partial, sizeof(double) * 2 * es::kMaxTChunk * es::kIntegrateBlocks);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_sigma, sizeof(double) * 2 * es::kMaxTChunk);
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_sigma, sizeof(double) * 2 * es::kMaxTChunk);
@@ -372,6 +378,22 @@ es_status es_destroy(es_ctx* ctx)
 }
 
 const char* es_last_error(const es_ctx* ctx) { return ctx ? ctx->err : g_create_error; }
+
+es_status es_get_tuning(const es_ctx* ctx, es_tuning* out)
+{
+    if (!ctx || !out) return ES_ERR_BAD_ARG;
+    *out = ctx->tuning;
+    return ES_OK;
+}
+
+es_status es_set_tuning(es_ctx* ctx, const es_tuning* tuning)
+{
+    if (!ctx || !tuning) return ES_ERR_BAD_ARG;
+    if (tuning->lifetime_variant < 0 || tuning->lifetime_variant >= es::kLifetimeVariants)
+        return fail(ctx, ES_ERR_BAD_ARG, "unknown lifetime variant %d", tuning->lifetime_variant);
+    ctx->tuning = *tuning;
+    return ES_OK;
+}
 
 es_status es_upload_grid(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
                          const es_impurity_settings* is, uint64_t generation)

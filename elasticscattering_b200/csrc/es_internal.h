@@ -55,6 +55,16 @@ struct LifetimeLaunch {
     long long n_orbits;
     int cpr, dim, n_phase, clockwise, coherent, walk_cap;
     int row0;                     // first start-position row of this launch
+    int variant;                  // LifetimeVariant
+    unsigned long long* work;     // refill variant: orbit counter, zeroed by the launcher
+};
+
+enum LifetimeVariant : int {
+    kLifetimePerThread = 0,      // one orbit per thread, <= 80 registers (3 blocks of 256 per SM)
+    kLifetimeRefill = 1,         // persistent warps, lanes refill as their orbits finish, 2 blocks per SM
+    kLifetimePerThreadLean = 2,  // one orbit per thread, <= 64 registers (4 blocks per SM)
+    kLifetimeRefillLean = 3,     // lane refill, <= 85 registers (3 blocks per SM)
+    kLifetimeVariants = 4
 };
 
 constexpr int kIntegrateBlocks = 296;   // 2 x 148 SMs; fixed so the reduction order is fixed

@@ -128,17 +128,15 @@ __device__ __forceinline__ double first_cross_time(const OrbitD& o, dv2 ip, doub
     const dv2 p1 = {o.center.x + ux * xs + uy * ys, o.center.y + uy * xs + -ux * ys};
     const dv2 p2 = {o.center.x + ux * xs + -uy * ys, o.center.y + uy * xs + ux * ys};
 
-    const double phi1 = get_angle(p1, o);
-    const double phi2 = get_angle(p2, o);
-
+    // Crossing point 1, then 2 (the order of the reference's min updates).
     double t_min = kINF;
-    if (angle_in_range(phi1, vr_x, vr_y, o.clockwise)) {
-        const double t = cross_angle(o.particle_angle, phi1, o.clockwise) / w;
-        t_min = (t_min < t) ? t_min : t;
-    }
-    if (angle_in_range(phi2, vr_x, vr_y, o.clockwise)) {
-        const double t = cross_angle(o.particle_angle, phi2, o.clockwise) / w;
-        t_min = (t_min < t) ? t_min : t;
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        const double phi_k = get_angle(k == 0 ? p1 : p2, o);
+        if (angle_in_range(phi_k, vr_x, vr_y, o.clockwise)) {
+            const double t = cross_angle(o.particle_angle, phi_k, o.clockwise) / w;
+            t_min = (t_min < t) ? t_min : t;
+        }
     }
     return t_min;
 }
@@ -211,8 +209,13 @@ __device__ __forceinline__ void update_first_boundary(const OrbitD& o, int offx,
     const bool i2_valid = horizontal ? point_in_segment(i2.x, p1.x, p2.x) : point_in_segment(i2.y, p1.y, p2.y);
 
     const iv2 next_cell = {last.cell.x + offx, last.cell.y + offy};
-    if (i1_valid) update_best(o, i1, next_cell, last, closest, L);
-    if (i2_valid) update_best(o, i2, next_cell, last, closest, L);
+    // i1 then i2, as the reference; one loop body keeps a single inlined copy
+    // of GetAngle (asin) instead of two per edge.
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        const bool valid = k == 0 ? i1_valid : i2_valid;
+        if (valid) update_best(o, k == 0 ? i1 : i2, next_cell, last, closest, L);
+    }
 }
 
 // GetNextCell, cell_grid.h:132-181
@@ -227,10 +230,16 @@ __device__ __forceinline__ bool next_cell(const OrbitD& o, double phi, const Gri
     const dv2 tr = {ll.x + L, ll.y + L};
     const dv2 tl = {ll.x + 0.0, ll.y + L};
 
-    update_first_boundary(o, 0, 1, tl, tr, L, last, next);
-    update_first_boundary(o, 0, -1, ll, lr, L, last, next);
-    update_first_boundary(o, 1, 0, lr, tr, L, last, next);
-    update_first_boundary(o, -1, 0, ll, tl, L, last, next);
+    // Edges in the reference's order: top (tl->tr), bottom (ll->lr),
+    // right (lr->tr), left (ll->tl). One loop body, one inlined copy.
+#pragma unroll 1
+    for (int e = 0; e < 4; e++) {
+        const dv2 p1 = e == 0 ? tl : (e == 2 ? lr : ll);
+        const dv2 p2 = e == 0 ? tr : (e == 1 ? lr : (e == 2 ? tr : tl));
+        const int offx = e < 2 ? 0 : (e == 2 ? 1 : -1);
+        const int offy = e == 0 ? 1 : (e == 1 ? -1 : 0);
+        update_first_boundary(o, offx, offy, p1, p2, L, last, next);
+    }
 
     {
         const double delta = 1e-7 * L;

@@ -1,0 +1,73 @@
+"""One sector pass of a named workload, for profiling or timing a kernel.
+
+    python -m elasticscattering_b200.profile_pass --workload config1 --field 20 --coherent 0 [--passes 1]
+        [--variant V] [--time]
+
+Builds the workload's impurity field on the host, uploads it, and runs
+`--passes` lifetime passes (stage a) followed by one integration (stages b, c),
+then prints the pass metrics as JSON. Meant to run under `ncu -k <kernel> -c 1`.
+With --time, every pass is timed with CUDA events on the context stream and
+each lifetime variant's lifetimes are compared bit for bit.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+from . import Grid, SimulationCUDA, make_settings, workloads
+from . import _native as N
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="config1", choices=sorted(workloads.WORKLOADS))
+    ap.add_argument("--field", type=float, default=20.0)
+    ap.add_argument("--coherent", type=int, default=0)
+    ap.add_argument("--passes", type=int, default=1)
+    ap.add_argument("--precision", type=int, default=N.ES_PRECISION_FP64)
+    ap.add_argument("--variant", type=int, default=None, help="lifetime kernel variant (default: library default)")
+    ap.add_argument("--time", action="store_true", help="time every variant with CUDA events")
+    a = ap.parse_args()
+    w = workloads.WORKLOADS[a.workload]()
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    s = make_settings(w.tau, w.alpha, w.clockwise, w.particle_speed, w.region_size, w.region_extends, w.density,
+                      w.impurity_radius, w.target_cell_population)
+    with SimulationCUDA(w.dim, w.phi_steps, g.info(), precision=a.precision) as sim:
+        sim.InitSample(g, s, bool(a.coherent))
+        if a.variant is not None:
+            sim.set_tuning(lifetime_variant=a.variant)
+        if a.time:
+            import torch
+            stream = torch.cuda.ExternalStream(sim.stream_handle())
+            report = {}
+            ref = None
+            for variant in (0, 1, 2, 3):
+                sim.set_tuning(lifetime_variant=variant)
+                ms = []
+                for _ in range(a.passes + 1):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    N.check(N.cuda_lib().es_enqueue_lifetimes(sim.ctx, a.field), sim.ctx)
+                    e1.record(stream)
+                    sim.synchronize()
+                    ms.append(e0.elapsed_time(e1))
+                lt, m = sim.ComputeLifetimes(a.field)
+                same = None if ref is None else bool(np.array_equal(ref.view(np.int64), lt.view(np.int64)))
+                ref = lt if ref is None else ref
+                report[f"variant{variant}"] = {"ms": [round(x, 3) for x in ms[1:]], "bitwise_equal_to_v0": same}
+            print(json.dumps({"workload": w.name, "field": a.field, "coherent": a.coherent, "timing": report}))
+            return
+        for _ in range(a.passes):
+            N.check(N.cuda_lib().es_enqueue_lifetimes(sim.ctx, a.field), sim.ctx)
+        sim.synchronize()
+        m = sim.read_metrics(reset=True)
+        sig = sim.DeriveTemperatures(np.array(w.temperatures))
+    print(json.dumps({"workload": w.name, "field": a.field, "coherent": a.coherent, "orbits": w.orbits_per_pass,
+                      "metrics": m, "sigma": [(x.xx, x.xy) for x in sig]}))
+
+
+if __name__ == "__main__":
+    main()

@@ -260,6 +260,18 @@ class SimulationCUDA:
         self._check(N.cuda_lib().es_read_metrics(self._ctx, C.byref(m), 1 if reset else 0))
         return m.as_dict()
 
+    def get_tuning(self) -> dict:
+        t = N.Tuning()
+        self._check(N.cuda_lib().es_get_tuning(self._ctx, C.byref(t)))
+        return {name: int(getattr(t, name)) for name, _ in N.Tuning._fields_}
+
+    def set_tuning(self, **fields) -> None:
+        t = N.Tuning()
+        self._check(N.cuda_lib().es_get_tuning(self._ctx, C.byref(t)))
+        for k, v in fields.items():
+            setattr(t, k, int(v))
+        self._check(N.cuda_lib().es_set_tuning(self._ctx, C.byref(t)))
+
     def stream_handle(self) -> int:
         return int(N.cuda_lib().es_stream(self._ctx) or 0)
 

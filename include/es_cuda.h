@@ -97,12 +97,24 @@ typedef struct es_sim_desc {
 
 typedef struct es_ctx es_ctx;
 
+/* Kernel choices of a context. No reference counterpart (the reference's
+ * OpenCL launch shape is fixed, src/sim/SimulationCL.cpp:412-431); the
+ * autotuner picks these, the defaults are the measured best on B200. */
+typedef struct es_tuning {
+    int32_t lifetime_variant;  /* 0 = one orbit per thread, 1 = persistent warps with lane refill,
+                                  2 / 3 = the same two with a tighter register budget */
+} es_tuning;
+
 /* Replaces SimulationCL::SimulationCL (src/sim/SimulationCL.cpp:386-475): binds a
  * device, creates the stream and the per-pass buffers. */
 es_status es_create(const es_sim_desc* desc, es_ctx** out);
 
 /* Replaces SimulationCL::~SimulationCL (src/sim/SimulationCL.cpp:477-508). */
 es_status es_destroy(es_ctx* ctx);
+
+/* Reads / sets the kernel choices of a context (see es_tuning). */
+es_status es_get_tuning(const es_ctx* ctx, es_tuning* out);
+es_status es_set_tuning(es_ctx* ctx, const es_tuning* tuning);
 
 /* Message of the last failure on this context ("" if none). ctx may be NULL
  * for failures of es_create. */

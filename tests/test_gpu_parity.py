@@ -228,6 +228,21 @@ def test_lifetime_known_answers_on_device(cuda_device, golden):
                         (c["name"], v, op, val)
 
 
+@pytest.mark.parametrize("coherent", [True, False])
+def test_lifetime_variants_agree_bitwise(config0_setup, coherent):
+    """The per-thread and lane-refill kernels schedule orbits differently but run
+    the same arithmetic: lifetimes and every metric counter are identical."""
+    w, g, og, sim = config0_setup
+    sim.InitSample(g, settings_of(w), coherent)
+    runs = {}
+    for variant in (0, 1):
+        sim.set_tuning(lifetime_variant=variant)
+        runs[variant] = sim.ComputeLifetimes(5.0)
+    sim.set_tuning(lifetime_variant=1)
+    assert np.array_equal(runs[0][0].view(np.int64), runs[1][0].view(np.int64))
+    assert runs[0][1] == runs[1][1]
+
+
 def test_results_are_bit_reproducible(config0_setup):
     w, g, og, sim = config0_setup
     sim.InitSample(g, settings_of(w), False)
@@ -303,7 +318,10 @@ def test_config1_full_size_rows_and_properties(cuda_device):
         for coh in (True, False):
             sim.InitSample(g, settings_of(w), coh)
             lt, m = sim.ComputeLifetimes(B)
-            assert m["particles_escaped"] == 0 and (lt >= 0).all()
+            # The reference counts an orbit as escaped whenever GetNextCell makes no
+            # progress (src/sim/es/cell_grid.h:177-180), e.g. grazing a cell edge, so
+            # a handful occur at this size even with a large region extension.
+            assert m["particles_escaped"] <= 1e-6 * w.orbits_per_pass and (lt >= 0).all()
             bt = bound_times(w, coh, B)
             if bt is not None:
                 assert (lt <= bt).all()
