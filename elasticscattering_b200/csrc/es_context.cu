@@ -83,7 +83,7 @@ struct es_ctx {
     int64_t pos_cap = 0;
     double last_w = 0;                // angular speed of the resident lifetimes
     unsigned long long* d_work = nullptr;  // orbit counter of the refill kernel
-    es_tuning tuning{es::kLifetimePerThreadLean};
+    es_tuning tuning{es::kLifetimePerThreadDefer};
     bool lifetimes_valid = false;
 };
 

@@ -64,7 +64,10 @@ enum LifetimeVariant : int {
     kLifetimeRefill = 1,         // persistent warps, lanes refill as their orbits finish, 2 blocks per SM
     kLifetimePerThreadLean = 2,  // one orbit per thread, <= 64 registers (4 blocks per SM)
     kLifetimeRefillLean = 3,     // lane refill, <= 85 registers (3 blocks per SM)
-    kLifetimeVariants = 4
+    kLifetimePositionMajor = 4,  // as 2, lanes = neighbouring start positions at one phase
+    kLifetimePositionMajorDefer = 5,  // as 4, crossing computations deferred past the cheap tests
+    kLifetimePerThreadDefer = 6,      // as 2, crossing computations deferred past the cheap tests
+    kLifetimeVariants = 7
 };
 
 constexpr int kIntegrateBlocks = 296;   // 2 x 148 SMs; fixed so the reduction order is fixed

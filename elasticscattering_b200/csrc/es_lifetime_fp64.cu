@@ -51,19 +51,37 @@ __device__ __forceinline__ void warp_flush(unsigned long long* metrics, unsigned
     }
 }
 
-template <int kMinBlocks>
+// kPositionMajor = false: lanes take consecutive orbits of the storage order,
+// i.e. 32 phases of one start position. kPositionMajor = true: lanes take 32
+// neighbouring start positions of one row at the same phase; their orbits are
+// parallel shifts of each other (by the position spacing, a fraction of a
+// cell), so they cross the same cells and edges and scan the same impurity
+// lists, which keeps the warp converged. Stores are then strided.
+template <int kMinBlocks, bool kPositionMajor, int kDefer>
 __global__ void __launch_bounds__(256, kMinBlocks) lifetime_fp64_kernel(LifetimeLaunch P)
 {
+    __shared__ int s_defer[kDefer > 0 ? kDefer * kDeferStride : 1];
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = t < P.n_orbits;
     const unsigned mask = __ballot_sync(0xffffffffu, active);
     if (!active) return;
 
-    const long long g = (long long)P.row0 * P.dim * P.n_phase + t;
-    const int v = (int)(g % P.n_phase);
-    const long long pidx = g / P.n_phase;
-    const int i = (int)(pidx % P.dim);
-    const int j = (int)(pidx / P.dim);
+    int v, i, j;
+    long long g;
+    if (kPositionMajor) {
+        // t = ((row * n_phase) + v) * dim + i over the rows of this launch
+        i = (int)(t % P.dim);
+        const long long rv = t / P.dim;
+        v = (int)(rv % P.n_phase);
+        j = P.row0 + (int)(rv / P.n_phase);
+        g = ((long long)j * P.dim + i) * P.n_phase + v;
+    } else {
+        g = (long long)P.row0 * P.dim * P.n_phase + t;
+        v = (int)(g % P.n_phase);
+        const long long pidx = g / P.n_phase;
+        i = (int)(pidx % P.dim);
+        j = (int)(pidx / P.dim);
+    }
 
     // Simulation position grid, src/sim/SimulationCPU.cpp:114:
     // v2(i, j) * distance_between_positions + small_offset
@@ -103,7 +121,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) lifetime_fp64_kernel(Lifetime
     if (!within_bounds(c0, gr.cpr)) {
         atomicOr(P.error, kErrStartCell);
     } else {
-        lt = trace_orbit(o, position, ph.phi, P.w, gr, P.walk_cap, cnt, flags);
+        lt = trace_orbit<kDefer>(o, position, ph.phi, P.w, gr, P.walk_cap, cnt, flags, s_defer + threadIdx.x);
         if (flags & kTraceWalkCap) atomicOr(P.error, kErrWalkCap);
     }
     P.out[g] = lt;
@@ -406,11 +424,11 @@ cudaError_t launch_refill(const LifetimeLaunch& L, cudaStream_t s)
     return cudaGetLastError();
 }
 
-template <int kMinBlocks>
+template <int kMinBlocks, bool kPositionMajor, int kDefer>
 cudaError_t launch_per_thread(const LifetimeLaunch& L, cudaStream_t s)
 {
     const long long blocks = (L.n_orbits + 255) / 256;
-    lifetime_fp64_kernel<kMinBlocks><<<(unsigned)blocks, 256, 0, s>>>(L);
+    lifetime_fp64_kernel<kMinBlocks, kPositionMajor, kDefer><<<(unsigned)blocks, 256, 0, s>>>(L);
     return cudaGetLastError();
 }
 
@@ -420,10 +438,13 @@ cudaError_t launch_lifetimes_fp64(const LifetimeLaunch& L, cudaStream_t s)
 {
     if (L.n_orbits <= 0) return cudaSuccess;
     switch (L.variant) {
-        case kLifetimePerThread: return launch_per_thread<3>(L, s);
+        case kLifetimePerThread: return launch_per_thread<3, false, 0>(L, s);
         case kLifetimeRefill: return launch_refill<2>(L, s);
-        case kLifetimePerThreadLean: return launch_per_thread<4>(L, s);
+        case kLifetimePerThreadLean: return launch_per_thread<4, false, 0>(L, s);
         case kLifetimeRefillLean: return launch_refill<3>(L, s);
+        case kLifetimePositionMajor: return launch_per_thread<4, true, 0>(L, s);
+        case kLifetimePositionMajorDefer: return launch_per_thread<4, true, 4>(L, s);
+        case kLifetimePerThreadDefer: return launch_per_thread<4, false, 4>(L, s);
         default: return cudaErrorInvalidValue;
     }
 }

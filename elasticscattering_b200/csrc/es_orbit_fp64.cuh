@@ -276,8 +276,20 @@ enum TraceFlag : int { kTraceOk = 0, kTraceInside = 1, kTraceEscaped = 2, kTrace
 // angle, `w` the unsigned angular speed. The loop is bounded by walk_cap cell
 // steps (the reference loops while(1)); exceeding it flags kTraceWalkCap and
 // returns 0.
+//
+// kDefer > 0: the cell's impurity scan first runs the cheap CirclesCross test
+// over all impurities and parks the indices of crossing ones in `defer`
+// (kDefer slots per thread, stride kDeferStride ints, shared memory); the
+// expensive GetFirstCrossTime then runs over the parked indices only. A warp
+// then executes the expensive branch about max-over-lanes(crossings) times per
+// cell instead of once per impurity position that any lane crosses. The
+// lifetime is a min over the same set of crossing times, so the result is
+// identical.
+constexpr int kDeferStride = 256;
+
+template <int kDefer = 0>
 __device__ __forceinline__ double trace_orbit(const OrbitD& o, dv2 position, double phi, double w, const GridD& g,
-                                              int walk_cap, OrbitCounters& cnt, int& flags)
+                                              int walk_cap, OrbitCounters& cnt, int& flags, int* defer = nullptr)
 {
     double lifetime = kINF;
     Isect next;
@@ -313,12 +325,38 @@ __device__ __forceinline__ double trace_orbit(const OrbitD& o, dv2 position, dou
         cnt.cells += 1;
         cnt.imps += end - start;
 
-        for (int k = start; k < end; k++) {
-            const double2 imp = __ldg(g.imps + k);
-            const dv2 ip = {imp.x, imp.y};
-            if (circles_cross(o, ip, g.imp_r)) {
-                cnt.crossings += 1;
-                const double t = first_cross_time(o, ip, g.imp_r, w, vr_x, vr_y);
+        if (kDefer == 0) {
+            for (int k = start; k < end; k++) {
+                const double2 imp = __ldg(g.imps + k);
+                const dv2 ip = {imp.x, imp.y};
+                if (circles_cross(o, ip, g.imp_r)) {
+                    cnt.crossings += 1;
+                    const double t = first_cross_time(o, ip, g.imp_r, w, vr_x, vr_y);
+                    lifetime = (t < lifetime) ? t : lifetime;
+                }
+            }
+        } else {
+            int parked = 0;
+            for (int k = start; k < end; k++) {
+                const double2 imp = __ldg(g.imps + k);
+                if (circles_cross(o, dv2{imp.x, imp.y}, g.imp_r)) {
+                    cnt.crossings += 1;
+                    defer[parked * kDeferStride] = k;
+                    if (++parked == kDefer) {
+#pragma unroll 1
+                        for (int c = 0; c < parked; c++) {
+                            const double2 pi = __ldg(g.imps + defer[c * kDeferStride]);
+                            const double t = first_cross_time(o, dv2{pi.x, pi.y}, g.imp_r, w, vr_x, vr_y);
+                            lifetime = (t < lifetime) ? t : lifetime;
+                        }
+                        parked = 0;
+                    }
+                }
+            }
+#pragma unroll 1
+            for (int c = 0; c < parked; c++) {
+                const double2 pi = __ldg(g.imps + defer[c * kDeferStride]);
+                const double t = first_cross_time(o, dv2{pi.x, pi.y}, g.imp_r, w, vr_x, vr_y);
                 lifetime = (t < lifetime) ? t : lifetime;
             }
         }

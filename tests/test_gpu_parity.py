@@ -234,13 +234,15 @@ def test_lifetime_variants_agree_bitwise(config0_setup, coherent):
     the same arithmetic: lifetimes and every metric counter are identical."""
     w, g, og, sim = config0_setup
     sim.InitSample(g, settings_of(w), coherent)
+    default = sim.get_tuning()
     runs = {}
-    for variant in (0, 1):
+    for variant in range(7):
         sim.set_tuning(lifetime_variant=variant)
         runs[variant] = sim.ComputeLifetimes(5.0)
-    sim.set_tuning(lifetime_variant=1)
-    assert np.array_equal(runs[0][0].view(np.int64), runs[1][0].view(np.int64))
-    assert runs[0][1] == runs[1][1]
+    sim.set_tuning(**default)
+    for variant in range(1, 7):
+        assert np.array_equal(runs[0][0].view(np.int64), runs[variant][0].view(np.int64)), variant
+        assert runs[0][1] == runs[variant][1], variant
 
 
 def test_results_are_bit_reproducible(config0_setup):
