@@ -37,6 +37,7 @@ CUDA_UNITS = {
     "es_lifetime_fp64.cu": ["-fmad=false"],
     "es_integrate.cu": ["-fmad=false"],
     "es_probe.cu": [],
+    "es_noalloc.cu": ["-fmad=false"],
 }
 
 HOST_UNITS = ["grid.cpp", "config.cpp", "logger.cpp", "simulation_cuda.cpp", "runner.cpp"]

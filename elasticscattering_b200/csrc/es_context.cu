@@ -379,6 +379,12 @@ es_status es_destroy(es_ctx* ctx)
 
 const char* es_last_error(const es_ctx* ctx) { return ctx ? ctx->err : g_create_error; }
 
+}  // extern "C"
+
+void es::set_global_error(const char* msg) { snprintf(g_create_error, sizeof g_create_error, "%s", msg ? msg : ""); }
+
+extern "C" {
+
 es_status es_get_tuning(const es_ctx* ctx, es_tuning* out)
 {
     if (!ctx || !out) return ES_ERR_BAD_ARG;

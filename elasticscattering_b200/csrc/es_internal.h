@@ -93,6 +93,9 @@ struct IntegrateLaunch {
     int n_blocks;                 // partial blocks per temperature
 };
 
+// Message returned by es_last_error(NULL), for entry points without a context.
+void set_global_error(const char* msg);
+
 cudaError_t launch_lifetimes_fp64(const LifetimeLaunch& L, cudaStream_t s);
 // Stages (b)+(c) for one temperature group: two launches.
 cudaError_t launch_integrate(const IntegrateLaunch& L, cudaStream_t s);

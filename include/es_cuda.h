@@ -117,7 +117,7 @@ es_status es_get_tuning(const es_ctx* ctx, es_tuning* out);
 es_status es_set_tuning(es_ctx* ctx, const es_tuning* tuning);
 
 /* Message of the last failure on this context ("" if none). ctx may be NULL
- * for failures of es_create. */
+ * for failures of es_create and es_derive_temperatures_noalloc. */
 const char* es_last_error(const es_ctx* ctx);
 
 /* Replaces the impurity/index upload in SimulationCL::ComputeLifetimes
@@ -205,6 +205,33 @@ es_status es_debug_next_cell(es_ctx* ctx, double center_x, double center_y, doub
 es_status es_debug_trace(es_ctx* ctx, double px, double py, int32_t q, int32_t p, double magnetic_field,
                          double phi_start, double phi_step_size, double alpha, double particle_speed,
                          int32_t is_clockwise, int32_t is_coherent, double* out_lifetime);
+
+/* Stages (b)+(c) -- the phase and start-position Simpson integrals of
+ * es_derive_temperatures -- without allocating any device memory. No
+ * counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: a framework that owns all device
+ * memory through its own pool, or a path on which a driver allocation (and its
+ * implicit synchronisation) is not allowed. The caller passes the raw lifetimes
+ * of one sector pass (d_lifetimes, device memory, dim^2 * 4 * phi_steps doubles
+ * in [j][i][q][p] order, e.g. as es_compute_lifetimes returns them), the
+ * sector's settings, field and temperatures, and d_out_sigma (device memory,
+ * 2 * n_t doubles: xx, xy per temperature). Work is enqueued on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) and not waited for.
+ *
+ * The scratch (phase table and block partial sums) is one fixed array of
+ * 169 KB that every GPU which loads this library holds until the process
+ * exits. Limit: phi_steps <= 1025; larger values return ES_ERR_BAD_ARG with a
+ * message in es_last_error(NULL). The first call on a device (with that device
+ * current) looks up the array's device address; make it before any stream
+ * capture. Every call shares the array and leaves its contents behind; each
+ * call rewrites every slot it reads before reading it, so nothing needs
+ * clearing between calls, but calls whose work overlaps on the GPU (different
+ * streams, or threads) race on it. */
+es_status es_derive_temperatures_noalloc(const double* d_lifetimes, int32_t positions_per_row, int32_t phi_steps,
+                                         const es_settings* s, int32_t coherent, double magnetic_field,
+                                         const double* temperatures, int32_t n_t, double* d_out_sigma,
+                                         void* stream);
 
 /* Measured FP64 FMA throughput of a device (TFLOP/s, 2 FLOP per FMA): the
  * denominator of the lifetime kernel's roofline. No reference counterpart
