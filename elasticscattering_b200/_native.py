@@ -49,7 +49,7 @@ class Metrics(C.Structure):
                 ("particles_inside_impurity", C.c_int64), ("particles_escaped", C.c_int64),
                 ("particles_at_bound", C.c_int64), ("max_impurities_tested", C.c_int64),
                 ("max_cells_passed", C.c_int64), ("crossings_tested", C.c_int64),
-                ("start_cell_tests", C.c_int64)]
+                ("start_cell_tests", C.c_int64), ("retraced_fp64", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {name: int(getattr(self, name)) for name, _ in self._fields_}

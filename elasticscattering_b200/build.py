@@ -37,6 +37,9 @@ CUDA_UNITS = {
     "es_lifetime_fp64.cu": ["-fmad=false"],
     "es_integrate.cu": ["-fmad=false"],
     "es_probe.cu": [],
+    # FP32 walk: contraction allowed; its FP64 parts (winner time, re-trace)
+    # call the same restated functions, so keep them uncontracted as well.
+    "es_lifetime_split.cu": ["-fmad=false"],
     "es_noalloc.cu": ["-fmad=false"],
 }
 

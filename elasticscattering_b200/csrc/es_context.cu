@@ -83,6 +83,12 @@ struct es_ctx {
     int64_t pos_cap = 0;
     double last_w = 0;                // angular speed of the resident lifetimes
     unsigned long long* d_work = nullptr;  // orbit counter of the refill kernel
+    // split precision
+    float2* d_imps32 = nullptr;            // cell-local FP32 impurities
+    int64_t imps32_cap = 0;
+    long long* d_retrace = nullptr;        // orbits for the FP64 re-trace
+    unsigned long long* d_retrace_count = nullptr;
+    long long retrace_cap = 0;
     es_tuning tuning{es::kLifetimePerThreadDefer};
     bool lifetimes_valid = false;
 };
@@ -181,6 +187,10 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.row0 = 0;
     L.variant = ctx->tuning.lifetime_variant;
     L.work = ctx->d_work;
+    L.imps32 = ctx->d_imps32;
+    L.retrace = ctx->d_retrace;
+    L.retrace_count = ctx->d_retrace_count;
+    L.retrace_cap = ctx->retrace_cap;
     return L;
 }
 
@@ -191,8 +201,13 @@ es_status enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
         return fail(ctx, ES_ERR_BAD_ARG, "magnetic field must be positive and finite (got %g)", magnetic_field);
     const es::LifetimeLaunch L =
         make_launch(ctx, magnetic_field, ctx->settings.particle_speed, ctx->settings.is_clockwise ? 1 : 0, ctx->coherent);
-    ES_CUDA(es::launch_lifetimes_fp64(L, ctx->stream), "lifetime kernel launch");
-    ctx->launches++;
+    if (ctx->desc.precision == ES_PRECISION_SPLIT) {
+        ES_CUDA(es::launch_lifetimes_split(L, ctx->stream), "split lifetime kernel launch");
+        ctx->launches += 2;
+    } else {
+        ES_CUDA(es::launch_lifetimes_fp64(L, ctx->stream), "lifetime kernel launch");
+        ctx->launches++;
+    }
     ctx->last_w = L.w;
     ctx->lifetimes_valid = true;
     return ES_OK;
@@ -244,6 +259,8 @@ es_status read_device_error(es_ctx* ctx)
     ES_CUDA(cudaStreamSynchronize(ctx->stream), "stream synchronize");
     if (h_err) {
         ES_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream), "error reset");
+        if (h_err & es::kErrRetraceOverflow)
+            return fail(ctx, ES_ERR_LAUNCH, "split precision: the FP64 re-trace list overflowed; results are invalid");
         if (h_err & es::kErrWalkCap)
             return fail(ctx, ES_ERR_WALK_CAP, "an orbit exceeded the cell-walk step bound (its lifetime was set to 0)");
         return fail(ctx, ES_ERR_BAD_ARG, "a start position lies outside the impurity grid");
@@ -267,6 +284,7 @@ es_status read_metrics_into(es_ctx* ctx, es_metrics* out, bool reset)
         out->max_cells_passed = (int64_t)h[es::kMetMaxCells];
         out->crossings_tested = (int64_t)h[es::kMetCrossings];
         out->start_cell_tests = (int64_t)h[es::kMetStartTests];
+        out->retraced_fp64 = (int64_t)h[es::kMetRetraced];
     }
     return ES_OK;
 }
@@ -299,6 +317,9 @@ void release(es_ctx* ctx)
     cudaFree(ctx->d_sigma);
     cudaFree(ctx->d_pos);
     cudaFree(ctx->d_work);
+    cudaFree(ctx->d_imps32);
+    cudaFree(ctx->d_retrace);
+    cudaFree(ctx->d_retrace_count);
     if (ctx->h_sigma) cudaFreeHost(ctx->h_sigma);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -354,6 +375,13 @@ es_status es_create(const es_sim_desc* desc, es_ctx** out)
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_metrics, sizeof(unsigned long long) * es::kMetCount);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_work, sizeof(unsigned long long));
+    if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT) {
+        // Re-traced orbits are a small fraction (guard-band decisions); a quarter
+        // of the pass is a generous bound, and overflow is reported, not ignored.
+        ctx->retrace_cap = ctx->n_orbits / 4 + 1024;
+        e = cudaMalloc(&ctx->d_retrace, sizeof(long long) * ctx->retrace_cap);
+        if (e == cudaSuccess) e = cudaMalloc(&ctx->d_retrace_count, sizeof(unsigned long long));
+    }
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_partial, sizeof(double) * 2 * es::kMaxTChunk * es::kIntegrateBlocks);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_sigma, sizeof(double) * 2 * es::kMaxTChunk);
     if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_sigma, sizeof(double) * 2 * es::kMaxTChunk);
@@ -443,6 +471,19 @@ es_status es_upload_grid(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, c
                 "impurity upload");
     ES_CUDA(cudaMemcpyAsync(ctx->d_cell_end, cell_end, sizeof(int) * n_cells, cudaMemcpyHostToDevice, ctx->stream),
             "cell index upload");
+    if (ctx->desc.precision == ES_PRECISION_SPLIT) {
+        if (n_indexed > ctx->imps32_cap) {
+            cudaFree(ctx->d_imps32);
+            ctx->d_imps32 = nullptr;
+            ctx->imps32_cap = 0;
+            ES_CUDA(cudaMalloc(&ctx->d_imps32, sizeof(float2) * (n_indexed > 0 ? n_indexed : 1)), "FP32 impurity buffer");
+            ctx->imps32_cap = n_indexed;
+        }
+        ES_CUDA(es::launch_local_impurities(ctx->d_imps, ctx->d_cell_end, ctx->d_imps32, is->spawn_region_start,
+                                            is->cell_size, is->cells_per_row, ctx->stream),
+                "FP32 impurity conversion");
+        ctx->launches++;
+    }
     ES_CUDA(cudaStreamSynchronize(ctx->stream), "grid upload");
     ctx->n_imps = n_indexed;
     ctx->is = *is;

@@ -19,11 +19,12 @@ enum MetricSlot : int {
     kMetMaxCells = 6,
     kMetCrossings = 7,
     kMetStartTests = 8,
-    kMetCount = 9
+    kMetRetraced = 9,
+    kMetCount = 10
 };
 
 // Device error bits (written with atomicOr, read by es_synchronize).
-enum DeviceError : int { kErrWalkCap = 1, kErrStartCell = 2 };
+enum DeviceError : int { kErrWalkCap = 1, kErrStartCell = 2, kErrRetraceOverflow = 4 };
 
 // Per-phase constants of one sector, tabulated on the host by es_init_sample
 // with the reference's expressions (CreateParticle, src/sim/es/lifetime.h:36-58):
@@ -57,6 +58,11 @@ struct LifetimeLaunch {
     int row0;                     // first start-position row of this launch
     int variant;                  // LifetimeVariant
     unsigned long long* work;     // refill variant: orbit counter, zeroed by the launcher
+    // split precision
+    const float2* imps32;         // cell-local FP32 copy of imps
+    long long* retrace;           // orbits handed to the FP64 re-trace
+    unsigned long long* retrace_count;
+    long long retrace_cap;
 };
 
 enum LifetimeVariant : int {
@@ -97,6 +103,10 @@ struct IntegrateLaunch {
 void set_global_error(const char* msg);
 
 cudaError_t launch_lifetimes_fp64(const LifetimeLaunch& L, cudaStream_t s);
+// Split precision: FP32 walk, then the FP64 re-trace of the listed orbits (two launches).
+cudaError_t launch_lifetimes_split(const LifetimeLaunch& L, cudaStream_t s);
+cudaError_t launch_local_impurities(const double2* imps, const int* cell_end, float2* out, double start, double cell,
+                                    int cpr, cudaStream_t s);
 // Stages (b)+(c) for one temperature group: two launches.
 cudaError_t launch_integrate(const IntegrateLaunch& L, cudaStream_t s);
 cudaError_t launch_debug_trace(const LifetimeLaunch& L, const PhaseOrbit& ph, double px, double py, double* d_out,

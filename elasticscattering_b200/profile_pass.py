@@ -29,7 +29,11 @@ def main() -> None:
     ap.add_argument("--precision", type=int, default=N.ES_PRECISION_FP64)
     ap.add_argument("--variant", type=int, default=None, help="lifetime kernel variant (default: library default)")
     ap.add_argument("--time", action="store_true", help="time every variant with CUDA events")
+    ap.add_argument("--compare-split", action="store_true", help="time plain FP64 against split precision")
     a = ap.parse_args()
+    if a.compare_split:
+        compare_split(a)
+        return
     w = workloads.WORKLOADS[a.workload]()
     g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
                        w.target_cell_population)
@@ -67,6 +71,40 @@ def main() -> None:
         sig = sim.DeriveTemperatures(np.array(w.temperatures))
     print(json.dumps({"workload": w.name, "field": a.field, "coherent": a.coherent, "orbits": w.orbits_per_pass,
                       "metrics": m, "sigma": [(x.xx, x.xy) for x in sig]}))
+
+
+def compare_split(a) -> None:
+    import torch
+    w = workloads.WORKLOADS[a.workload]()
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    s = make_settings(w.tau, w.alpha, w.clockwise, w.particle_speed, w.region_size, w.region_extends, w.density,
+                      w.impurity_radius, w.target_cell_population)
+    res = {}
+    lts = {}
+    for name, prec in (("fp64", N.ES_PRECISION_FP64), ("split", N.ES_PRECISION_SPLIT)):
+        with SimulationCUDA(w.dim, w.phi_steps, g.info(), precision=prec) as sim:
+            sim.InitSample(g, s, bool(a.coherent))
+            stream = torch.cuda.ExternalStream(sim.stream_handle())
+            ms = []
+            for _ in range(a.passes + 1):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                N.check(N.cuda_lib().es_enqueue_lifetimes(sim.ctx, a.field), sim.ctx)
+                e1.record(stream)
+                sim.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            sim.read_metrics(reset=True)
+            lt, m = sim.ComputeLifetimes(a.field)
+            lts[name] = lt
+            res[name] = {"ms": [round(x, 3) for x in ms[1:]], "retraced": m["retraced_fp64"]}
+    x, y = lts["fp64"], lts["split"]
+    nz = (x != 0) & (y != 0)
+    res["flips"] = int(((x == 0) != (y == 0)).sum())
+    res["bit_identical"] = float((x.view(np.int64) == y.view(np.int64)).mean())
+    res["max_rel"] = float((np.abs(x[nz] - y[nz]) / np.abs(x[nz])).max()) if nz.any() else 0.0
+    print(json.dumps({"workload": w.name, "field": a.field, "coherent": a.coherent, "orbits": w.orbits_per_pass,
+                      **res}))
 
 
 if __name__ == "__main__":

@@ -81,6 +81,7 @@ typedef struct es_metrics {
     int64_t max_cells_passed;
     int64_t crossings_tested; /* orbit/impurity pairs that passed CirclesCross (FLOP model) */
     int64_t start_cell_tests; /* InsideImpurity tests of the start-cell scans (FLOP model) */
+    int64_t retraced_fp64;    /* split precision: orbits re-traced by the FP64 kernel */
 } es_metrics;
 
 /* Constructor arguments of Simulation (src/sim/Simulation.h:131-146) plus

@@ -1,0 +1,95 @@
+"""Split precision (ES_PRECISION_SPLIT) against the plain FP64 path, through the C ABI.
+
+North-star bar for the split path: sigma within 1e-6 relative of plain FP64, error stated
+per result. The split kernel recomputes every winning crossing with the reference's FP64
+arithmetic and re-traces in FP64 every orbit whose FP32 decisions lack margin, so the
+tests also hold it to the plain path's per-orbit bars: the same hit/no-hit/at-bound class
+for every orbit and lifetimes within 1e-9.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from elasticscattering_b200 import Grid, SimulationCUDA, make_settings, workloads
+from elasticscattering_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+SPLIT_SIGMA_RTOL = 1e-6
+LIFETIME_RTOL = 1e-9
+
+
+def settings_of(w):
+    return make_settings(w.tau, w.alpha, w.clockwise, w.particle_speed, w.region_size, w.region_extends,
+                         w.density, w.impurity_radius, w.target_cell_population)
+
+
+def pair(w, grid, device):
+    plain = SimulationCUDA(w.dim, w.phi_steps, grid.info(), device=device, precision=N.ES_PRECISION_FP64)
+    split = SimulationCUDA(w.dim, w.phi_steps, grid.info(), device=device, precision=N.ES_PRECISION_SPLIT)
+    return plain, split
+
+
+def compare(a: np.ndarray, b: np.ndarray) -> dict:
+    ca, cb = (a == 0), (b == 0)
+    flips = int((ca != cb).sum())
+    nz = ~ca & ~cb
+    rel = np.abs(a[nz] - b[nz]) / np.abs(a[nz])
+    return {"flips": flips, "max_rel": float(rel.max()) if rel.size else 0.0,
+            "bit_identical": float((a.view(np.int64) == b.view(np.int64)).mean())}
+
+
+@pytest.mark.parametrize("wname,fields", [("config0", (20.0, 5.0, 40.0)), ("config3", (40.0,))])
+def test_split_matches_plain_per_orbit(cuda_device, wname, fields):
+    w = workloads.WORKLOADS[wname]()
+    if wname == "config3":
+        w.dim, w.phi_steps = 129, 33  # the stress-case geometry at a test-sized start grid
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    plain, split = pair(w, g, cuda_device)
+    try:
+        for coherent in (True, False):
+            plain.InitSample(g, settings_of(w), coherent)
+            split.InitSample(g, settings_of(w), coherent)
+            for B in fields:
+                a, ma = plain.ComputeLifetimes(B)
+                b, mb = split.ComputeLifetimes(B)
+                r = compare(a, b)
+                assert r["flips"] == 0 and r["max_rel"] <= LIFETIME_RTOL, (coherent, B, r, mb["retraced_fp64"])
+                assert mb["retraced_fp64"] < 0.05 * len(a)
+                for k in ("cells_passed", "impurities_tested", "crossings_tested", "particles_inside_impurity",
+                          "particles_escaped", "particles_at_bound"):
+                    assert ma[k] == mb[k], (coherent, B, k, ma[k], mb[k])
+                temps = [1e-3, 10.0, 40.0]
+                sa, sb = plain.DeriveTemperatures(temps), split.DeriveTemperatures(temps)
+                for x, y in zip(sa, sb):
+                    assert abs(x.xx - y.xx) <= SPLIT_SIGMA_RTOL * abs(x.xx)
+                    assert abs(x.xy - y.xy) <= SPLIT_SIGMA_RTOL * abs(x.xy)
+    finally:
+        plain.close()
+        split.close()
+
+
+def test_split_config1_full_size(cuda_device):
+    """config 1 at full size (34.08 M orbits per pass): every orbit compared with the plain path."""
+    w = workloads.config1()
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    plain, split = pair(w, g, cuda_device)
+    try:
+        for coherent in (True, False):
+            plain.InitSample(g, settings_of(w), coherent)
+            split.InitSample(g, settings_of(w), coherent)
+            for B in (1.0, 20.0):
+                a, _ = plain.ComputeLifetimes(B)
+                b, mb = split.ComputeLifetimes(B)
+                r = compare(a, b)
+                assert r["flips"] == 0 and r["max_rel"] <= LIFETIME_RTOL, (coherent, B, r, mb["retraced_fp64"])
+                sa = plain.DeriveTemperatures([1e-3])[0]
+                sb = split.DeriveTemperatures([1e-3])[0]
+                assert abs(sa.xx - sb.xx) <= SPLIT_SIGMA_RTOL * abs(sa.xx)
+                assert abs(sa.xy - sb.xy) <= SPLIT_SIGMA_RTOL * abs(sa.xy)
+    finally:
+        plain.close()
+        split.close()
