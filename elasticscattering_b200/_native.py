@@ -87,6 +87,7 @@ CUDA_API = {
     "es_stream": (_vp, [_vp]),
     "es_launch_count": (_i64, [_vp]),
     "es_probe_fp64_fma": (_i32, [_i32, C.POINTER(_d)]),
+    "es_probe_fp32_fma": (_i32, [_i32, C.POINTER(_d)]),
     "es_derive_temperatures_noalloc": (_i32, [_vp, _i32, _i32, C.POINTER(Settings), _i32, _d, _vp, _i32, _vp, _vp]),
     "es_debug_trace": (_i32, [_vp, _d, _d, _i32, _i32, _d, _d, _d, _d, _d, _i32, _i32, C.POINTER(_d)]),
     "es_debug_next_cell": (_i32, [_vp, _d, _d, _d, _i32, _d, C.POINTER(ImpuritySettings), _vp, _vp,

@@ -41,6 +41,74 @@ __device__ __forceinline__ float wrap2pi(float a) { return a - kTwoPiF * floorf(
 // Advance (angle travelled since the start, in [0, 2pi)) of position angle psi.
 __device__ __forceinline__ float advance(float psi, float psi0, float dir) { return wrap2pi(dir * (psi - psi0)); }
 
+// atan(t) for t in [0, 1] as t * P(t^2), a least-squares polynomial fitted
+// for this kernel (max abs error 1.2e-7 rad evaluated in FP32).
+__device__ __forceinline__ float atan_unit(float t)
+{
+    const float z = t * t;
+    float p = 0.0024682495277374983f;
+    p = fmaf(p, z, -0.01445870939642191f);
+    p = fmaf(p, z, 0.03989958390593529f);
+    p = fmaf(p, z, -0.07247953116893768f);
+    p = fmaf(p, z, 0.10507321357727051f);
+    p = fmaf(p, z, -0.14164334535598755f);
+    p = fmaf(p, z, 0.19986537098884583f);
+    p = fmaf(p, z, -0.3333265781402588f);
+    p = fmaf(p, z, 0.9999998807907104f);
+    return t * p;
+}
+
+// atan2 by octant reduction onto atan_unit; (0, 0) never reaches it.
+__device__ __forceinline__ float fast_atan2(float y, float x)
+{
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float a0 = atan_unit(__fdividef(fminf(ax, ay), fmaxf(ax, ay)));
+    float a = ay > ax ? 0.5f * kPiF - a0 : a0;
+    a = x < 0.0f ? kPiF - a : a;
+    return copysignf(a, y);
+}
+
+// 2 asin(sqrt(s2)): the crossing half-angle, a series for the usual tiny s2.
+__device__ __forceinline__ float half_angle(float s2)
+{
+    const float x = sqrtf(s2);
+    if (s2 < 0.01f) {
+        // asin(x) = x (1 + z/6 + 3 z^2/40 + 5 z^3/112 + ...), z = x^2
+        const float p = fmaf(fmaf(fmaf(0.044642857142857144f, s2, 0.075f), s2, 0.16666666666666666f), s2, 1.0f);
+        return 2.0f * x * p;
+    }
+    return 2.0f * fast_atan2(x, sqrtf(1.0f - s2));
+}
+
+// The two crossing advances of the circle (radius r, centre at the origin)
+// with an edge line at signed distance c64 (x = c for vertical lines, y = c for
+// horizontal ones); both -1 when the line misses the circle. acos(|c| / r) is
+// taken as atan2(sqrt(m (2 - m)), 1 - m) with m = (r - |c|) / r from FP64, which
+// stays accurate near tangency.
+__device__ __forceinline__ void line_crossings(double c64, double r64, float inv_r, bool horizontal, float psi0,
+                                               float dir, float& a1, float& a2)
+{
+    const double m64 = r64 - fabs(c64);
+    if (!(m64 > 0.0)) {
+        a1 = a2 = -1.0f;
+        return;
+    }
+    const float m = (float)m64 * inv_r;
+    const float ths = fast_atan2(sqrtf(m * (2.0f - m)), 1.0f - m);  // acos(|u|)
+    float p1, p2;
+    if (!horizontal) {
+        const float acu = c64 >= 0.0 ? ths : kPiF - ths;
+        p1 = acu;
+        p2 = -acu;
+    } else {
+        const float asu = c64 >= 0.0 ? (0.5f * kPiF - ths) : (ths - 0.5f * kPiF);
+        p1 = asu;
+        p2 = kPiF - asu;
+    }
+    a1 = advance(p1, psi0, dir);
+    a2 = advance(p2, psi0, dir);
+}
+
 // FP64 GetFirstCrossTime without the valid-range filter, as an angle: the
 // earlier of the two crossings' GetCrossAngle (src/sim/es/details.h:153-206).
 // Divided by w this is the reference's time for the disk that holds the first
@@ -99,11 +167,17 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
     const double L = P.cell_size;
     const int cpr = P.cpr;
     const double r64 = o.radius;
-    const float r = (float)r64;
-    const float inv2r = 0.5f / r;
     const double ir64 = P.imp_radius;
+    const float r = (float)r64;
+    const float inv_r = (float)(1.0 / r64);
     const float ir = (float)ir64;
-    const float band = 1e-3f * ir;  // |d - r| within this of ir: CirclesCross decided in FP64
+    // CirclesCross in d^2: anything outside [lo2 - eps2, hi2 + eps2] misses for
+    // sure (the FP32 d^2 error is below 3e-7 r^2); inside, |d - r| decides, and
+    // within band_d of the edge the decision and the angle are taken in FP64.
+    const float lo2 = (float)((r64 - ir64) * (r64 - ir64)), hi2 = (float)((r64 + ir64) * (r64 + ir64));
+    const float eps2 = 2e-6f * r * r;
+    const float band_d = 0.02f * ir;
+    const float inv4r = 0.25f * inv_r;
     // Position angle of the start: C = pos -/+ r (sin phi, -cos phi) (details.h:243-250).
     const float dir = o.clockwise ? -1.0f : 1.0f;
     const float psi0 = (float)(o.clockwise ? o.particle_angle - kHALF_PI : o.particle_angle + kHALF_PI);
@@ -122,7 +196,7 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
         for (int k = k0; k < k1; k++) {
             const float2 q = __ldg(P.imps32 + k);
             const float dx = plx - q.x, dy = ply - q.y;
-            const float d2 = dx * dx + dy * dy;
+            const float d2 = fmaf(dx, dx, dy * dy);
             cnt.start_tests += 1;
             bool inside = d2 < ir2;
             if (fabsf(d2 - ir2) <= 1e-4f * ir2) {
@@ -137,8 +211,21 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
         }
     }
 
-    float a_cur = 0.0f;      // advance at which the current cell was entered
-    int entry_line = -1;     // edge line crossed to enter (0 x-lo, 1 x-hi, 2 y-lo, 3 y-hi)
+    // Crossing advances of the current cell's four edge lines (x-lo, x-hi,
+    // y-lo, y-hi), two per line, -1 when the line misses the circle. Moving to
+    // a neighbour keeps three of the four lines, so one line is new per step.
+    float la[4], lb[4];
+    const double llx0 = P.spawn_start + cx * L, lly0 = P.spawn_start + cy * L;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const double c64 = e == 0 ? llx0 - o.center.x
+                                  : (e == 1 ? (llx0 + L) - o.center.x
+                                            : (e == 2 ? lly0 - o.center.y : (lly0 + L) - o.center.y));
+        line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+    }
+
+    float a_cur = 0.0f;        // advance at which the current cell was entered
+    int entry_line = -1;       // edge line crossed to enter
     float global_a = 3.0e38f;  // earliest disk crossing seen in any visited cell
     int steps = 0;
 
@@ -149,26 +236,10 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
         float ex = kTwoPiF, ex2 = kTwoPiF;
         int ex_line = -1, ex2_line = -1;
         bool ambiguous = false;
-#pragma unroll 1
+#pragma unroll
         for (int e = 0; e < 4; e++) {
-            const double c64 = e == 0 ? llx - o.center.x
-                                      : (e == 1 ? (llx + L) - o.center.x
-                                                : (e == 2 ? lly - o.center.y : (lly + L) - o.center.y));
-            const double m64 = r64 - fabs(c64);  // distance of the line inside the circle
-            if (!(m64 > 0.0)) continue;
-            // acos(|u|) with u = c / r, well conditioned near tangency
-            const float ths = 2.0f * asinf(sqrtf((float)m64 * inv2r));
-            float p1, p2;
-            if (e < 2) {
-                const float acu = c64 >= 0.0 ? ths : kPiF - ths;
-                p1 = acu;
-                p2 = -acu;
-            } else {
-                const float asu = c64 >= 0.0 ? (0.5f * kPiF - ths) : (ths - 0.5f * kPiF);
-                p1 = asu;
-                p2 = kPiF - asu;
-            }
-            float a1 = advance(p1, psi0, dir), a2 = advance(p2, psi0, dir);
+            float a1 = la[e], a2 = lb[e];
+            if (a1 < 0.0f) continue;
             if (e == entry_line) {
                 // one of the two is the entry crossing itself
                 const float d1 = fabsf(a1 - a_cur), d2 = fabsf(a2 - a_cur);
@@ -220,10 +291,12 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
         for (int k = k0; k < k1; k++) {
             const float2 q = __ldg(P.imps32 + k);
             const float dx = q.x + ox, dy = q.y + oy;
-            const float d = sqrtf(dx * dx + dy * dy);
+            const float d2 = fmaf(dx, dx, dy * dy);
+            if (d2 < lo2 - eps2 || d2 > hi2 + eps2) continue;
+            const float d = d2 * rsqrtf(d2);
             const float delta = d - r;
             float a;
-            if (fabsf(fabsf(delta) - ir) <= band) {
+            if (fabsf(fabsf(delta) - ir) <= band_d) {
                 // grazing disk: CirclesCross and the crossing angle in FP64
                 const double2 q64 = __ldg(P.imps + k);
                 if (!circles_cross(o, dv2{q64.x, q64.y}, ir64)) continue;
@@ -232,12 +305,12 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
                 if (!(fabsf(delta) < ir)) continue;
                 // crossing half-angle at the orbit centre:
                 // sin^2(beta / 2) = (ir - delta)(ir + delta) / (4 d r)
-                const float s2 = (ir - delta) * (ir + delta) / (4.0f * d * r);
-                const float beta = 2.0f * asinf(sqrtf(s2));
+                const float s2 = __fdividef((ir - delta) * (ir + delta) * inv4r, d);
+                const float beta = half_angle(s2);
                 // The disk's arc on the orbit is [ac - beta, ac + beta] in advance;
                 // one that touches the start angle is left to FP64 (taking the min
                 // of two separately wrapped FP32 advances could pick the wrong end).
-                const float ac = advance(atan2f(dy, dx), psi0, dir);
+                const float ac = advance(fast_atan2(dy, dx), psi0, dir);
                 if (ac - beta < kGuard || ac + beta > kTwoPiF - kGuard) return kSplitRetrace;
                 a = ac - beta;
             }
@@ -260,10 +333,22 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
 
         if (!final_visit && !(global_a < ex + kGuard)) {
             if (++steps >= P.walk_cap) return kSplitRetrace;
-            entry_line = ex_line ^ 1;  // entering across the opposite line of the neighbour
-            a_cur = ex;
+            // Enter the neighbour: the crossed line becomes its opposite line,
+            // the parallel line moves by one cell, the other two are shared.
+            entry_line = ex_line ^ 1;
+            la[entry_line] = la[ex_line];
+            lb[entry_line] = lb[ex_line];
             cx = nx;
             cy = ny;
+            {
+                const double nllx = P.spawn_start + cx * L, nlly = P.spawn_start + cy * L;
+                const int e = ex_line;  // the new cell's line on the far side has the same index
+                const double c64 = e == 0 ? nllx - o.center.x
+                                          : (e == 1 ? (nllx + L) - o.center.x
+                                                    : (e == 2 ? nlly - o.center.y : (nlly + L) - o.center.y));
+                line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+            }
+            a_cur = ex;
             continue;
         }
         // This visit ends the walk: a crossing at or before the exit (or the

@@ -1,6 +1,7 @@
-// es_probe.cu - measured FP64 pipe rate: the denominator of the stage (a)
-// roofline. Independent FP64 FMA chains, enough warps to cover the DFMA
-// latency on every SM, timed with CUDA events on a private stream.
+// es_probe.cu - measured FMA pipe rates: the denominators of the stage (a)
+// rooflines (FP64 for the plain kernel, FP32 for the split kernel's bulk).
+// Independent FMA chains, enough warps to cover the FMA latency on every SM,
+// timed with CUDA events on a private stream.
 #include "es_cuda.h"
 
 #include <cuda_runtime.h>
@@ -10,24 +11,24 @@ namespace {
 constexpr int kChains = 8;
 constexpr int kIters = 2048;
 
-__global__ void __launch_bounds__(256) fp64_fma_kernel(double* sink, double a, double b)
+template <typename T>
+__global__ void __launch_bounds__(256) fma_kernel(T* sink, T a, T b)
 {
-    double x[kChains];
+    T x[kChains];
 #pragma unroll
-    for (int c = 0; c < kChains; c++) x[c] = (double)(threadIdx.x + c) * 1e-3;
+    for (int c = 0; c < kChains; c++) x[c] = (T)(threadIdx.x + c) * (T)1e-3;
     for (int i = 0; i < kIters; i++) {
 #pragma unroll
         for (int c = 0; c < kChains; c++) x[c] = fma(x[c], a, b);
     }
-    double s = 0.0;
+    T s = 0;
 #pragma unroll
     for (int c = 0; c < kChains; c++) s += x[c];
-    if (s == 12345.678) sink[0] = s;  // keeps the chains live
+    if (s == (T)12345.678) sink[0] = s;  // keeps the chains live
 }
 
-}  // namespace
-
-extern "C" es_status es_probe_fp64_fma(int32_t device_ordinal, double* out_tflops)
+template <typename T>
+es_status probe(int32_t device_ordinal, double* out_tflops)
 {
     if (!out_tflops) return ES_ERR_BAD_ARG;
     if (cudaSetDevice(device_ordinal) != cudaSuccess) return ES_ERR_DEVICE;
@@ -35,17 +36,17 @@ extern "C" es_status es_probe_fp64_fma(int32_t device_ordinal, double* out_tflop
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal);
     cudaStream_t s;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return ES_ERR_LAUNCH;
-    double* sink = nullptr;
+    T* sink = nullptr;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     es_status st = ES_OK;
-    if (cudaMalloc(&sink, sizeof(double)) != cudaSuccess) st = ES_ERR_OOM;
+    if (cudaMalloc(&sink, sizeof(T)) != cudaSuccess) st = ES_ERR_OOM;
     const int blocks = sms * 8;
     float best_ms = 1e30f;
     for (int rep = 0; st == ES_OK && rep < 5; rep++) {
         cudaEventRecord(e0, s);
-        fp64_fma_kernel<<<blocks, 256, 0, s>>>(sink, 0.999999, 1e-9);
+        fma_kernel<T><<<blocks, 256, 0, s>>>(sink, (T)0.999999, (T)1e-9);
         cudaEventRecord(e1, s);
         if (cudaEventSynchronize(e1) != cudaSuccess) st = ES_ERR_LAUNCH;
         float ms = 0;
@@ -61,4 +62,16 @@ extern "C" es_status es_probe_fp64_fma(int32_t device_ordinal, double* out_tflop
     cudaEventDestroy(e1);
     cudaStreamDestroy(s);
     return st;
+}
+
+}  // namespace
+
+extern "C" es_status es_probe_fp64_fma(int32_t device_ordinal, double* out_tflops)
+{
+    return probe<double>(device_ordinal, out_tflops);
+}
+
+extern "C" es_status es_probe_fp32_fma(int32_t device_ordinal, double* out_tflops)
+{
+    return probe<float>(device_ordinal, out_tflops);
 }

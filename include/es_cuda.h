@@ -239,6 +239,10 @@ es_status es_derive_temperatures_noalloc(const double* d_lifetimes, int32_t posi
  * (the reference publishes no device figures). Runs for a few milliseconds. */
 es_status es_probe_fp64_fma(int32_t device_ordinal, double* out_tflops);
 
+/* Measured FP32 FMA throughput (TFLOP/s): the denominator of the split
+ * kernel's roofline. No reference counterpart. */
+es_status es_probe_fp32_fma(int32_t device_ordinal, double* out_tflops);
+
 #ifdef __cplusplus
 }
 #endif
