@@ -1,0 +1,492 @@
+// es_orbit_split.cuh - stage (a), FP32/FP64 split precision: the per-orbit
+// walk shared by the single-pass kernel (es_lifetime_split.cu) and the batched
+// kernel (es_batch.cu).
+//
+// Same result as the plain FP64 kernel (the reference's TraceOrbit,
+// src/sim/es/lifetime.h:78-148) but with the bulk of the work in FP32:
+//
+// 1. The reference's walk returns the first crossing, along the orbit, of any
+//    impurity disk listed in the cells it visits before it stops: impurities
+//    are filed under every cell they overlap (src/sim/Grid.cpp:112-180), so a
+//    crossing point in a visited cell is always found in that visit. It stops
+//    after the first visit holding an accepted crossing, and it stops early
+//    (lifetime 0) when the next cell leaves the grid or the orbit comes full
+//    circle -- then only the last cell's disks count, over the rest of the
+//    circle (valid range [entry, start angle], lifetime.h:106).
+// 2. This kernel walks the same cells in FP32, in angle space relative to the
+//    orbit centre: the exit of a (convex) cell is the first crossing of any of
+//    its four edge lines. Disks are tested in FP32 on cell-local coordinates
+//    (CirclesCross decided in FP64 inside a tangency band) and their first
+//    crossing advance is kept in FP32.
+// 3. The winning disk's crossing time is then recomputed in FP64 with the
+//    reference's own GetCrossPoints/GetAngle/GetCrossAngle arithmetic, and
+//    clamped to the sector bound in FP64 -- the same bits as the plain path.
+// 4. Every decision that FP32 cannot settle with margin -- an exit within a
+//    guard angle of a corner, a cell arc shorter than the guard (where the
+//    reference's 1e-6 L DifferentPoint rule can stop the walk), a start point
+//    near an edge, two winners or a winner and an exit within the guard, the
+//    walk bound -- sends the whole orbit to a list that the plain FP64 kernel
+//    re-traces afterwards.
+#pragma once
+
+#include "es_internal.h"
+#include "es_orbit_fp64.cuh"
+
+namespace es {
+
+namespace {
+
+constexpr float kTwoPiF = 6.2831853071795864769f;
+constexpr float kPiF = 3.1415926535897932385f;
+constexpr float kGuard = 4e-6f;        // angle guard (rad): ~40x the FP32 angle error
+
+__device__ __forceinline__ float wrap2pi(float a) { return a - kTwoPiF * floorf(a * (1.0f / kTwoPiF)); }
+
+// Advance (angle travelled since the start, in [0, 2pi)) of position angle psi.
+__device__ __forceinline__ float advance(float psi, float psi0, float dir) { return wrap2pi(dir * (psi - psi0)); }
+
+// atan(t) for t in [0, 1] as t * P(t^2), a least-squares polynomial fitted
+// for this kernel (max abs error 1.2e-7 rad evaluated in FP32).
+__device__ __forceinline__ float atan_unit(float t)
+{
+    const float z = t * t;
+    float p = 0.0024682495277374983f;
+    p = fmaf(p, z, -0.01445870939642191f);
+    p = fmaf(p, z, 0.03989958390593529f);
+    p = fmaf(p, z, -0.07247953116893768f);
+    p = fmaf(p, z, 0.10507321357727051f);
+    p = fmaf(p, z, -0.14164334535598755f);
+    p = fmaf(p, z, 0.19986537098884583f);
+    p = fmaf(p, z, -0.3333265781402588f);
+    p = fmaf(p, z, 0.9999998807907104f);
+    return t * p;
+}
+
+// atan2 by octant reduction onto atan_unit; (0, 0) never reaches it.
+__device__ __forceinline__ float fast_atan2(float y, float x)
+{
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float a0 = atan_unit(__fdividef(fminf(ax, ay), fmaxf(ax, ay)));
+    float a = ay > ax ? 0.5f * kPiF - a0 : a0;
+    a = x < 0.0f ? kPiF - a : a;
+    return copysignf(a, y);
+}
+
+// 2 asin(sqrt(s2)): the crossing half-angle, a series for the usual tiny s2.
+__device__ __forceinline__ float half_angle(float s2)
+{
+    const float x = sqrtf(s2);
+    if (s2 < 0.01f) {
+        // asin(x) = x (1 + z/6 + 3 z^2/40 + 5 z^3/112 + ...), z = x^2
+        const float p = fmaf(fmaf(fmaf(0.044642857142857144f, s2, 0.075f), s2, 0.16666666666666666f), s2, 1.0f);
+        return 2.0f * x * p;
+    }
+    return 2.0f * fast_atan2(x, sqrtf(1.0f - s2));
+}
+
+// The two crossing advances of the circle (radius r, centre at the origin)
+// with an edge line at signed distance c64 (x = c for vertical lines, y = c for
+// horizontal ones); both -1 when the line misses the circle. acos(|c| / r) is
+// taken as atan2(sqrt(m (2 - m)), 1 - m) with m = (r - |c|) / r from FP64, which
+// stays accurate near tangency.
+__device__ __forceinline__ void line_crossings(double c64, double r64, float inv_r, bool horizontal, float psi0,
+                                               float dir, float& a1, float& a2)
+{
+    const double m64 = r64 - fabs(c64);
+    if (!(m64 > 0.0)) {
+        a1 = a2 = -1.0f;
+        return;
+    }
+    const float m = (float)m64 * inv_r;
+    const float ths = fast_atan2(sqrtf(m * (2.0f - m)), 1.0f - m);  // acos(|u|)
+    float p1, p2;
+    if (!horizontal) {
+        const float acu = c64 >= 0.0 ? ths : kPiF - ths;
+        p1 = acu;
+        p2 = -acu;
+    } else {
+        const float asu = c64 >= 0.0 ? (0.5f * kPiF - ths) : (ths - 0.5f * kPiF);
+        p1 = asu;
+        p2 = kPiF - asu;
+    }
+    a1 = advance(p1, psi0, dir);
+    a2 = advance(p2, psi0, dir);
+}
+
+// FP64 GetFirstCrossTime without the valid-range filter, as an angle: the
+// earlier of the two crossings' GetCrossAngle (src/sim/es/details.h:153-206).
+// Divided by w this is the reference's time for the disk that holds the first
+// crossing of the orbit.
+__device__ __forceinline__ double first_cross_angle_open(const OrbitD& o, dv2 ip, double ir)
+{
+    const double qx = o.center.x - ip.x;
+    const double qy = o.center.y - ip.y;
+    const double dist_sq = qx * qx + qy * qy;
+    const double dist = sqrt(dist_sq);
+    const double xs = (dist_sq + o.radius_sq - ir * ir) / (2.0 * dist);
+    const double ys = sqrt(o.radius_sq - xs * xs);
+    const double ux = (ip.x - o.center.x) / dist;
+    const double uy = (ip.y - o.center.y) / dist;
+    const dv2 p1 = {o.center.x + ux * xs + uy * ys, o.center.y + uy * xs + -ux * ys};
+    const dv2 p2 = {o.center.x + ux * xs + -uy * ys, o.center.y + uy * xs + ux * ys};
+    double a_min = kINF;
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        const double a = cross_angle(o.particle_angle, get_angle(k == 0 ? p1 : p2, o), o.clockwise);
+        a_min = (a_min < a) ? a_min : a;
+    }
+    return a_min;
+}
+
+enum SplitOutcome : int { kSplitDone = 0, kSplitRetrace = 1 };
+
+struct SplitCounters {
+    int cells, imps, crossings, start_tests;
+};
+
+// The winning disk's reference time (FP64) and the bound clamp.
+__device__ __forceinline__ double finish_hit(const LifetimeLaunch& P, const OrbitD& o, int win_k, int alt_k,
+                                             int& flags)
+{
+    const double2 q = __ldg(P.imps + win_k);
+    double t = first_cross_angle_open(o, dv2{q.x, q.y}, P.imp_radius) / P.w;
+    if (alt_k >= 0) {
+        const double2 a = __ldg(P.imps + alt_k);
+        const double t2 = first_cross_angle_open(o, dv2{a.x, a.y}, P.imp_radius) / P.w;
+        t = (t < t2) ? t : t2;
+    }
+    flags = kTraceOk;
+    if (t > o.bound_time) {  // lifetime.h:142-146
+        flags |= kTraceAtBound;
+        t = o.bound_time;
+    }
+    return t;
+}
+
+// FP32 walk of one orbit. Returns kSplitDone with `out` set (and flags for the
+// metrics), or kSplitRetrace when the orbit must be re-traced in FP64.
+__device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD& o, dv2 pos, SplitCounters& cnt,
+                                           int& flags, double& out)
+{
+    const double L = P.cell_size;
+    const int cpr = P.cpr;
+    const double r64 = o.radius;
+    const double ir64 = P.imp_radius;
+    const float r = (float)r64;
+    const float inv_r = (float)(1.0 / r64);
+    const float ir = (float)ir64;
+    // CirclesCross in d^2: anything outside [lo2 - eps2, hi2 + eps2] misses for
+    // sure (the FP32 d^2 error is below 3e-7 r^2); inside, |d - r| decides, and
+    // within band_d of the edge the decision and the angle are taken in FP64.
+    const float lo2 = (float)((r64 - ir64) * (r64 - ir64)), hi2 = (float)((r64 + ir64) * (r64 + ir64));
+    const float eps2 = 2e-6f * r * r;
+    const float band_d = 0.02f * ir;
+    const float inv4r = 0.25f * inv_r;
+    // Position angle of the start: C = pos -/+ r (sin phi, -cos phi) (details.h:243-250).
+    const float dir = o.clockwise ? -1.0f : 1.0f;
+    const float psi0 = (float)(o.clockwise ? o.particle_angle - kHALF_PI : o.particle_angle + kHALF_PI);
+
+    int cx = (int)((pos.x - P.spawn_start) / P.spawn_size * (double)cpr);
+    int cy = (int)((pos.y - P.spawn_start) / P.spawn_size * (double)cpr);
+
+    // Start-cell InsideImpurity scan (lifetime.h:90-99), FP32 with an FP64 band.
+    {
+        const int c = cy * cpr + cx;
+        const int k0 = (c == 0) ? 0 : __ldg(P.cell_end + c - 1);
+        const int k1 = __ldg(P.cell_end + c);
+        const float plx = (float)(pos.x - (P.spawn_start + cx * L));
+        const float ply = (float)(pos.y - (P.spawn_start + cy * L));
+        const float ir2 = ir * ir;
+        for (int k = k0; k < k1; k++) {
+            const float2 q = __ldg(P.imps32 + k);
+            const float dx = plx - q.x, dy = ply - q.y;
+            const float d2 = fmaf(dx, dx, dy * dy);
+            cnt.start_tests += 1;
+            bool inside = d2 < ir2;
+            if (fabsf(d2 - ir2) <= 1e-4f * ir2) {
+                const double2 q64 = __ldg(P.imps + k);
+                inside = inside_impurity(pos, dv2{q64.x, q64.y}, ir64);
+            }
+            if (inside) {
+                flags = kTraceInside;
+                out = 0.0;
+                return kSplitDone;
+            }
+        }
+    }
+
+    // Crossing advances of the current cell's four edge lines (x-lo, x-hi,
+    // y-lo, y-hi), two per line, -1 when the line misses the circle. Moving to
+    // a neighbour keeps three of the four lines, so one line is new per step.
+    float la[4], lb[4];
+    const double llx0 = P.spawn_start + cx * L, lly0 = P.spawn_start + cy * L;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const double c64 = e == 0 ? llx0 - o.center.x
+                                  : (e == 1 ? (llx0 + L) - o.center.x
+                                            : (e == 2 ? lly0 - o.center.y : (lly0 + L) - o.center.y));
+        line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+    }
+
+    float a_cur = 0.0f;        // advance at which the current cell was entered
+    int entry_line = -1;       // edge line crossed to enter
+    float global_a = 3.0e38f;  // earliest disk crossing seen in any visited cell
+    int steps = 0;
+
+    for (;;) {
+        const double llx = P.spawn_start + cx * L, lly = P.spawn_start + cy * L;
+
+        // ---- exit of this cell: first edge-line crossing after a_cur ----
+        float ex = kTwoPiF, ex2 = kTwoPiF;
+        int ex_line = -1, ex2_line = -1;
+        bool ambiguous = false;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            float a1 = la[e], a2 = lb[e];
+            if (a1 < 0.0f) continue;
+            if (e == entry_line) {
+                // one of the two is the entry crossing itself
+                const float d1 = fabsf(a1 - a_cur), d2 = fabsf(a2 - a_cur);
+                if (fminf(d1, kTwoPiF - d1) < fminf(d2, kTwoPiF - d2)) a1 = -1.0f; else a2 = -1.0f;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const float a = h == 0 ? a1 : a2;
+                if (a < 0.0f) continue;
+                if (fabsf(a - a_cur) < kGuard || a > kTwoPiF - kGuard) {
+                    ambiguous = true;  // crossing at the entry point (corner) or at the start angle
+                    continue;
+                }
+                if (a < a_cur) continue;
+                if (a < ex) {
+                    ex2 = ex;
+                    ex2_line = ex_line;
+                    ex = a;
+                    ex_line = e;
+                } else if (a < ex2) {
+                    ex2 = a;
+                    ex2_line = e;
+                }
+            }
+        }
+        if (ambiguous) return kSplitRetrace;
+        if (ex_line >= 0) {
+            if (ex - a_cur < kGuard) return kSplitRetrace;                                        // tiny arc
+            if (ex2_line >= 0 && ex2_line != ex_line && ex2 - ex < kGuard) return kSplitRetrace;  // corner
+        }
+        // Next cell across the exit line; a final visit when the orbit comes
+        // full circle or the next cell leaves the grid.
+        int nx = cx, ny = cy;
+        if (ex_line == 0) nx -= 1;
+        if (ex_line == 1) nx += 1;
+        if (ex_line == 2) ny -= 1;
+        if (ex_line == 3) ny += 1;
+        const bool final_visit = ex_line < 0 || nx < 0 || ny < 0 || nx >= cpr || ny >= cpr;
+
+        // ---- disks of this cell ----
+        const int c = cy * cpr + cx;
+        const int k0 = (c == 0) ? 0 : __ldg(P.cell_end + c - 1);
+        const int k1 = __ldg(P.cell_end + c);
+        cnt.cells += 1;
+        cnt.imps += k1 - k0;
+        const float ox = (float)(llx - o.center.x), oy = (float)(lly - o.center.y);
+        float v1 = 3.0e38f, v2 = 3.0e38f, v3 = 3.0e38f;  // best three crossing advances of this visit
+        int k1st = -1, k2nd = -1;
+        for (int k = k0; k < k1; k++) {
+            const float2 q = __ldg(P.imps32 + k);
+            const float dx = q.x + ox, dy = q.y + oy;
+            const float d2 = fmaf(dx, dx, dy * dy);
+            if (d2 < lo2 - eps2 || d2 > hi2 + eps2) continue;
+            const float d = d2 * rsqrtf(d2);
+            const float delta = d - r;
+            float a;
+            if (fabsf(fabsf(delta) - ir) <= band_d) {
+                // grazing disk: CirclesCross and the crossing angle in FP64
+                const double2 q64 = __ldg(P.imps + k);
+                if (!circles_cross(o, dv2{q64.x, q64.y}, ir64)) continue;
+                a = (float)first_cross_angle_open(o, dv2{q64.x, q64.y}, ir64);
+            } else {
+                if (!(fabsf(delta) < ir)) continue;
+                // crossing half-angle at the orbit centre:
+                // sin^2(beta / 2) = (ir - delta)(ir + delta) / (4 d r)
+                const float s2 = __fdividef((ir - delta) * (ir + delta) * inv4r, d);
+                const float beta = half_angle(s2);
+                // The disk's arc on the orbit is [ac - beta, ac + beta] in advance;
+                // one that touches the start angle is left to FP64 (taking the min
+                // of two separately wrapped FP32 advances could pick the wrong end).
+                const float ac = advance(fast_atan2(dy, dx), psi0, dir);
+                if (ac - beta < kGuard || ac + beta > kTwoPiF - kGuard) return kSplitRetrace;
+                a = ac - beta;
+            }
+            cnt.crossings += 1;
+            if (a < v1) {
+                v3 = v2;
+                v2 = v1;
+                k2nd = k1st;
+                v1 = a;
+                k1st = k;
+            } else if (a < v2) {
+                v3 = v2;
+                v2 = a;
+                k2nd = k;
+            } else if (a < v3) {
+                v3 = a;
+            }
+        }
+        global_a = fminf(global_a, v1);
+
+        if (!final_visit && !(global_a < ex + kGuard)) {
+            if (++steps >= P.walk_cap) return kSplitRetrace;
+            // Enter the neighbour: the crossed line becomes its opposite line,
+            // the parallel line moves by one cell, the other two are shared.
+            entry_line = ex_line ^ 1;
+            la[entry_line] = la[ex_line];
+            lb[entry_line] = lb[ex_line];
+            cx = nx;
+            cy = ny;
+            {
+                const double nllx = P.spawn_start + cx * L, nlly = P.spawn_start + cy * L;
+                const int e = ex_line;  // the new cell's line on the far side has the same index
+                const double c64 = e == 0 ? nllx - o.center.x
+                                          : (e == 1 ? (nllx + L) - o.center.x
+                                                    : (e == 2 ? nlly - o.center.y : (nlly + L) - o.center.y));
+                line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+            }
+            a_cur = ex;
+            continue;
+        }
+        // This visit ends the walk: a crossing at or before the exit (or the
+        // final visit). The reference accepts this cell's disks only, over
+        // [entry, exit] -- or over the rest of the circle in a final visit.
+        if (!final_visit && global_a > ex - kGuard) return kSplitRetrace;  // winner at the exit
+        if (k1st < 0) {
+            if (global_a < ex + kGuard) return kSplitRetrace;  // a crossing before the exit but not in this cell
+            flags = kTraceEscaped;                             // lifetime.h:131-136, then the bound check
+            out = 0.0;
+            if (out > o.bound_time) {
+                flags |= kTraceAtBound;
+                out = o.bound_time;
+            }
+            return kSplitDone;
+        }
+        if (global_a < v1 - kGuard) return kSplitRetrace;  // an earlier cell's crossing inside this visit
+        if (v3 < v1 + kGuard) return kSplitRetrace;         // three near-equal winners
+        // The first visit's valid range starts at, and a final visit's range ends
+        // at, the particle's raw phase angle (lifetime.h:84,106), which is
+        // negative for the incoherent sector's first quadrant. AngleInRange
+        // (details.h:119-136) then tests x and x + 2pi only and rejects some
+        // crossings the geometry accepts: clockwise in the final visit,
+        // counter-clockwise in the first. The FP64 walk reproduces that.
+        if (o.particle_angle < 0.0 && (o.clockwise ? final_visit : entry_line < 0)) return kSplitRetrace;
+        out = finish_hit(P, o, k1st, v2 < v1 + kGuard ? k2nd : -1, flags);
+        return kSplitDone;
+    }
+}
+
+// Orbit g of pass P (CreateParticle, src/sim/es/lifetime.h:36-58, with the
+// host-tabulated phase constants).
+__device__ __forceinline__ OrbitD make_orbit(const LifetimeLaunch& P, long long g, dv2& pos)
+{
+    const int v = (int)(g % P.n_phase);
+    const long long pidx = g / P.n_phase;
+    const int i = (int)(pidx % P.dim);
+    const int j = (int)(pidx / P.dim);
+    pos = dv2{(double)i * P.dist + P.off_x, (double)j * P.dist + P.off_y};
+    const PhaseOrbit ph = P.phase[v];
+    OrbitD o;
+    o.radius = P.radius;
+    o.radius_sq = P.radius_sq;
+    o.clockwise = P.clockwise != 0;
+    const double shift_x = (ph.vel_y * P.radius) / P.speed;
+    const double shift_y = (-ph.vel_x * P.radius) / P.speed;
+    o.center = o.clockwise ? dv2{pos.x - shift_x, pos.y - shift_y} : dv2{pos.x + shift_x, pos.y + shift_y};
+    o.bound_time = P.coherent ? kINF : ph.bound_dphi / P.w;
+    o.particle_angle = ph.phi;
+    return o;
+}
+
+// The split walk of orbit g. Returns true when the orbit must be re-traced in
+// FP64 (cnt and flags are then cleared); otherwise lt holds its lifetime.
+__device__ __forceinline__ bool split_orbit(const LifetimeLaunch& P, long long g, SplitCounters& cnt, int& flags,
+                                            double& lt)
+{
+    dv2 pos;
+    const OrbitD o = make_orbit(P, g, pos);
+    cnt = SplitCounters{0, 0, 0, 0};
+    flags = kTraceOk;
+    lt = 0.0;
+    const int cx = (int)((pos.x - P.spawn_start) / P.spawn_size * (double)P.cpr);
+    const int cy = (int)((pos.y - P.spawn_start) / P.spawn_size * (double)P.cpr);
+    if (cx < 0 || cy < 0 || cx >= P.cpr || cy >= P.cpr) {
+        atomicOr(P.error, kErrStartCell);
+        return false;
+    }
+    if (trace_split(P, o, pos, cnt, flags, lt) == kSplitRetrace) {
+        cnt = SplitCounters{0, 0, 0, 0};
+        flags = kTraceOk;
+        return true;
+    }
+    return false;
+}
+
+// Exact FP64 TraceOrbit of orbit g (src/sim/es/lifetime.h:78-148): writes the
+// lifetime and adds the orbit's metrics.
+__device__ __forceinline__ void retrace_orbit(const LifetimeLaunch& P, long long g)
+{
+    GridD gr;
+    gr.imps = P.imps;
+    gr.cell_end = P.cell_end;
+    gr.start = P.spawn_start;
+    gr.size = P.spawn_size;
+    gr.cell = P.cell_size;
+    gr.imp_r = P.imp_radius;
+    gr.cpr = P.cpr;
+    dv2 pos;
+    const OrbitD o = make_orbit(P, g, pos);
+    OrbitCounters cnt = {0, 0, 0, 0};
+    int flags = kTraceOk;
+    const double lt = trace_orbit(o, pos, o.particle_angle, P.w, gr, P.walk_cap, cnt, flags);
+    if (flags & kTraceWalkCap) atomicOr(P.error, kErrWalkCap);
+    P.out[g] = lt;
+    atomicAdd(P.metrics + kMetCells, (unsigned long long)cnt.cells);
+    atomicAdd(P.metrics + kMetImps, (unsigned long long)cnt.imps);
+    atomicAdd(P.metrics + kMetCrossings, (unsigned long long)cnt.crossings);
+    atomicAdd(P.metrics + kMetStartTests, (unsigned long long)cnt.start_tests);
+    if (flags & kTraceInside) atomicAdd(P.metrics + kMetInside, 1ull);
+    if (flags & kTraceEscaped) atomicAdd(P.metrics + kMetEscaped, 1ull);
+    if (flags & kTraceAtBound) atomicAdd(P.metrics + kMetAtBound, 1ull);
+    atomicMax(P.metrics + kMetMaxCells, (unsigned long long)cnt.cells);
+    atomicMax(P.metrics + kMetMaxImps, (unsigned long long)cnt.imps);
+    atomicAdd(P.metrics + kMetRetraced, 1ull);
+}
+
+// Metrics of the lanes in `mask` (one instance), one atomic per warp and counter.
+__device__ __forceinline__ void flush_split_metrics(unsigned long long* metrics, unsigned mask, const SplitCounters& cnt,
+                                                    int flags, bool live)
+{
+    const unsigned l = live ? 1u : 0u;
+    const unsigned s_cells = __reduce_add_sync(mask, (unsigned)cnt.cells);
+    const unsigned s_imps = __reduce_add_sync(mask, (unsigned)cnt.imps);
+    const unsigned s_cross = __reduce_add_sync(mask, (unsigned)cnt.crossings);
+    const unsigned s_start = __reduce_add_sync(mask, (unsigned)cnt.start_tests);
+    const unsigned s_inside = __reduce_add_sync(mask, (flags & kTraceInside) ? l : 0u);
+    const unsigned s_escaped = __reduce_add_sync(mask, (flags & kTraceEscaped) ? l : 0u);
+    const unsigned s_bound = __reduce_add_sync(mask, (flags & kTraceAtBound) ? l : 0u);
+    const unsigned m_cells = __reduce_max_sync(mask, (unsigned)cnt.cells);
+    const unsigned m_imps = __reduce_max_sync(mask, (unsigned)cnt.imps);
+    if ((threadIdx.x & 31) == (__ffs(mask) - 1)) {
+        if (s_cells) atomicAdd(metrics + kMetCells, (unsigned long long)s_cells);
+        if (s_imps) atomicAdd(metrics + kMetImps, (unsigned long long)s_imps);
+        if (s_cross) atomicAdd(metrics + kMetCrossings, (unsigned long long)s_cross);
+        if (s_start) atomicAdd(metrics + kMetStartTests, (unsigned long long)s_start);
+        if (s_inside) atomicAdd(metrics + kMetInside, (unsigned long long)s_inside);
+        if (s_escaped) atomicAdd(metrics + kMetEscaped, (unsigned long long)s_escaped);
+        if (s_bound) atomicAdd(metrics + kMetAtBound, (unsigned long long)s_bound);
+        if (m_cells) atomicMax(metrics + kMetMaxCells, (unsigned long long)m_cells);
+        if (m_imps) atomicMax(metrics + kMetMaxImps, (unsigned long long)m_imps);
+    }
+}
+
+}  // namespace
+
+}  // namespace es
