@@ -60,6 +60,22 @@ class Tuning(C.Structure):
     _fields_ = [("lifetime_variant", C.c_int32)]
 
 
+ES_BATCH_MAX_T = 8
+
+
+class BatchInstance(C.Structure):
+    """es_batch_instance: one (sample, field, sector) pass of a batch."""
+    _fields_ = [("grid", C.c_int32), ("positions_per_row", C.c_int32), ("particles_per_quadrant", C.c_int32),
+                ("coherent", C.c_int32), ("region_size", C.c_double), ("grid_cell_size", C.c_double),
+                ("magnetic_field", C.c_double), ("settings", Settings), ("n_t", C.c_int32),
+                ("temperatures", C.c_double * ES_BATCH_MAX_T)]
+
+
+class BatchTuning(C.Structure):
+    """es_batch_tuning: launch choices of a batch."""
+    _fields_ = [("chunk_iters", C.c_int32), ("blocks_per_sm", C.c_int32), ("precision", C.c_int32)]
+
+
 class SimDesc(C.Structure):
     _fields_ = [("positions_per_row", C.c_int32), ("particles_per_quadrant", C.c_int32),
                 ("region_size", C.c_double), ("region_extends", C.c_double), ("grid_cell_size", C.c_double),
@@ -89,6 +105,20 @@ CUDA_API = {
     "es_probe_fp64_fma": (_i32, [_i32, C.POINTER(_d)]),
     "es_probe_fp32_fma": (_i32, [_i32, C.POINTER(_d)]),
     "es_derive_temperatures_noalloc": (_i32, [_vp, _i32, _i32, C.POINTER(Settings), _i32, _d, _vp, _i32, _vp, _vp]),
+    "es_batch_create": (_i32, [_i32, C.POINTER(_vp)]),
+    "es_batch_destroy": (_i32, [_vp]),
+    "es_batch_last_error": (C.c_char_p, [_vp]),
+    "es_batch_get_tuning": (_i32, [_vp, C.POINTER(BatchTuning)]),
+    "es_batch_set_tuning": (_i32, [_vp, C.POINTER(BatchTuning)]),
+    "es_batch_add_grid": (_i32, [_vp, _vp, _i64, _vp, C.POINTER(ImpuritySettings), C.POINTER(_i32)]),
+    "es_batch_clear": (_i32, [_vp]),
+    "es_batch_set_instances": (_i32, [_vp, C.POINTER(BatchInstance), _i32]),
+    "es_batch_run": (_i32, [_vp, _vp, _vp]),
+    "es_batch_enqueue": (_i32, [_vp]),
+    "es_batch_collect": (_i32, [_vp, _vp, _vp]),
+    "es_batch_stream": (_vp, [_vp]),
+    "es_batch_launch_count": (_i64, [_vp]),
+    "es_batch_total_orbits": (_i64, [_vp]),
     "es_debug_trace": (_i32, [_vp, _d, _d, _i32, _i32, _d, _d, _d, _d, _d, _i32, _i32, C.POINTER(_d)]),
     "es_debug_next_cell": (_i32, [_vp, _d, _d, _d, _i32, _d, C.POINTER(ImpuritySettings), _vp, _vp,
                                   C.POINTER(_i32)]),
@@ -141,6 +171,12 @@ def host_lib() -> C.CDLL:
 def check(status: int, ctx=None) -> None:
     if status != ES_OK:
         msg = cuda_lib().es_last_error(ctx)
+        raise EsError(status, msg.decode() if msg else "")
+
+
+def check_batch(status: int, batch) -> None:
+    if status != ES_OK:
+        msg = cuda_lib().es_batch_last_error(batch)
         raise EsError(status, msg.decode() if msg else "")
 
 

@@ -41,6 +41,7 @@ CUDA_UNITS = {
     # call the same restated functions, so keep them uncontracted as well.
     "es_lifetime_split.cu": ["-fmad=false"],
     "es_noalloc.cu": ["-fmad=false"],
+    "es_batch.cu": ["-fmad=false"],
 }
 
 HOST_UNITS = ["grid.cpp", "config.cpp", "logger.cpp", "simulation_cuda.cpp", "runner.cpp"]

@@ -7,6 +7,7 @@
 // without FMA contraction (-Xcompiler -ffp-contract=off) and uses the host libm,
 // exactly like the reference's CPU code.
 #include "es_cuda.h"
+#include "es_host_math.h"
 #include "es_internal.h"
 
 #include <cfloat>
@@ -19,28 +20,9 @@
 
 namespace {
 
-// src/sim/es/constants.h:23-35
-constexpr double kM0 = 9.10938188e-31;
-constexpr double kM = (5.0 * kM0);
-constexpr double kE = 1.60217646e-19;
-constexpr double kHBAR = 1.05457148e-34;
-constexpr double kC1 = 1.15e-9;
-constexpr double kKB = 1.380649e-23;
-constexpr double kPI = 3.141592653589793238463;
-constexpr double kPI2 = 6.283185307179586;
-constexpr double kHALF_PI = 1.570796326794896619231;
+using es::host::kHALF_PI;
 
 thread_local char g_create_error[512] = "";
-
-double smod_h(double a, double b) { return a - b * std::floor(a / b); }
-
-// SimpsonWeight, src/sim/es/util.h:24-28
-double simpson_weight_h(int i, int dim)
-{
-    const double main_multiplier = (i % 2 == 0) ? 2.0 : 4.0;
-    const bool is_edge = (i == 0) || i == (dim - 1);
-    return is_edge ? 1.0 : main_multiplier;
-}
 
 }  // namespace
 
@@ -124,26 +106,15 @@ es_status bind(es_ctx* ctx)
     return ES_OK;
 }
 
-// GetSigmaIntegrandFactor with SigmaFactor inlined, src/sim/Simulation.h:69-76,88
 double integrand_factor(const es_ctx* ctx, double w, double tau)
 {
-    const double kf = kM * ctx->settings.particle_speed / kHBAR;
-    double outside = (kE * kE * kf * kf) / (2.0 * kPI * kPI * kM * kC1);
-    const double wct = w * tau;
-    outside *= tau / (1.0 + wct * wct);
-    return std::pow(1.0 / (3.0 * (ctx->desc.positions_per_row - 1)), 2) * ctx->phi_integrand_factor * outside * 1e-8;
+    return es::host::integrand_factor(ctx->settings.particle_speed, ctx->desc.positions_per_row,
+                                      ctx->phi_integrand_factor, w, tau);
 }
 
-// GetTau, src/sim/Simulation.h:90
 double get_tau(const es_ctx* ctx, double temperature)
 {
-    return ctx->coherent ? ctx->settings.tau : kHBAR / (kKB * temperature);
-}
-
-int walk_cap_for(double radius, double cell)
-{
-    const double steps = 4.0 * std::ceil(kPI2 * radius / cell) + 16.0;
-    return steps > 2.0e9 ? 2000000000 : (int)steps;
+    return es::host::get_tau(ctx->coherent != 0, ctx->settings.tau, temperature);
 }
 
 es_status check_ready(es_ctx* ctx)
@@ -157,7 +128,7 @@ es_status check_ready(es_ctx* ctx)
 es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double speed, int clockwise, int coherent)
 {
     // SimulationCPU::ComputeLifetimes, src/sim/SimulationCPU.cpp:107-108
-    const double w = kE * magnetic_field / kM;
+    const double w = es::host::angular_speed(magnetic_field);
     es::LifetimeLaunch L{};
     L.imps = ctx->d_imps;
     L.cell_end = ctx->d_cell_end;
@@ -183,7 +154,7 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.n_phase = ctx->n_phase;
     L.clockwise = clockwise;
     L.coherent = coherent;
-    L.walk_cap = walk_cap_for(L.radius, L.cell_size);
+    L.walk_cap = es::host::walk_cap_for(L.radius, L.cell_size);
     L.row0 = 0;
     L.variant = ctx->tuning.lifetime_variant;
     L.work = ctx->d_work;
@@ -525,35 +496,15 @@ es_status es_init_sample(es_ctx* ctx, const es_settings* s, int32_t coherent)
 
     // Simulation::InitSample, src/sim/Simulation.h:111-126
     const int ppq = ctx->desc.particles_per_quadrant;
-    const double base_area = s->alpha * 2.0;
-    ctx->area = !coherent ? base_area : (kHALF_PI - base_area);
-    ctx->phi_integrand_factor = ctx->area / ((ppq - 1) * 3.0);
-    ctx->phi_start = (!coherent ? -s->alpha : s->alpha);
-    ctx->phi_step = ctx->area / (ppq - 1);
+    const es::host::Sector sec = es::host::sector(s->alpha, ppq, coherent != 0);
+    ctx->area = sec.area;
+    ctx->phi_integrand_factor = sec.phi_integrand_factor;
+    ctx->phi_start = sec.phi_start;
+    ctx->phi_step = sec.phi_step;
 
     std::vector<es::PhaseOrbit> po((size_t)ctx->n_phase);
     std::vector<es::PhaseSigma> psg((size_t)ctx->n_phase);
-    const bool clockwise = s->is_clockwise != 0;
-    for (int q = 0; q < 4; q++) {
-        for (int p = 0; p < ppq; p++) {
-            const int v = q * ppq + p;
-            // CreateParticle, src/sim/es/lifetime.h:39-45
-            const double phi = ctx->phi_start + q * kHALF_PI + p * ctx->phi_step;
-            es::PhaseOrbit& o = po[(size_t)v];
-            o.phi = phi;
-            o.vel_x = std::cos(phi) * s->particle_speed;
-            o.vel_y = std::sin(phi) * s->particle_speed;
-            // GetBoundTime's angle (is_future = false), src/sim/es/details.h:219-228
-            const double remaining = smod_h(phi + s->alpha, kHALF_PI);
-            o.bound_dphi = clockwise ? remaining : (2.0 * s->alpha - remaining);
-            // ApplySigma / IntegrateResult, src/sim/SimulationCPU.cpp:186-192,218
-            es::PhaseSigma& g = psg[(size_t)v];
-            g.phi = phi;
-            g.cos_phi = std::cos(phi);
-            g.sin_phi = std::sin(phi);
-            g.weight = simpson_weight_h(p, ppq);
-        }
-    }
+    es::host::phase_tables(sec, ppq, s->particle_speed, s->alpha, s->is_clockwise != 0, po.data(), psg.data());
     ES_CUDA(cudaMemcpyAsync(ctx->d_phase_orbit, po.data(), sizeof(es::PhaseOrbit) * po.size(), cudaMemcpyHostToDevice,
                             ctx->stream),
             "phase table upload");
@@ -689,7 +640,7 @@ es_status es_debug_trace(es_ctx* ctx, double px, double py, int32_t q, int32_t p
     ph.phi = phi_start + q * kHALF_PI + p * phi_step_size;
     ph.vel_x = std::cos(ph.phi) * particle_speed;
     ph.vel_y = std::sin(ph.phi) * particle_speed;
-    const double remaining = smod_h(ph.phi + alpha, kHALF_PI);
+    const double remaining = es::host::smod(ph.phi + alpha, kHALF_PI);
     ph.bound_dphi = is_clockwise ? remaining : (2.0 * alpha - remaining);
     double* d = nullptr;
     ES_CUDA(cudaMalloc(&d, sizeof(double)), "debug buffer");

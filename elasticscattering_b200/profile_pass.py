@@ -30,9 +30,15 @@ def main() -> None:
     ap.add_argument("--variant", type=int, default=None, help="lifetime kernel variant (default: library default)")
     ap.add_argument("--time", action="store_true", help="time every variant with CUDA events")
     ap.add_argument("--compare-split", action="store_true", help="time plain FP64 against split precision")
+    ap.add_argument("--batch", action="store_true",
+                    help="run the pass through the batched kernel (one instance, fused integration)")
+    ap.add_argument("--chunk-iters", type=int, default=32)
     a = ap.parse_args()
     if a.compare_split:
         compare_split(a)
+        return
+    if a.batch:
+        batch_pass(a)
         return
     w = workloads.WORKLOADS[a.workload]()
     g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
@@ -71,6 +77,35 @@ def main() -> None:
         sig = sim.DeriveTemperatures(np.array(w.temperatures))
     print(json.dumps({"workload": w.name, "field": a.field, "coherent": a.coherent, "orbits": w.orbits_per_pass,
                       "metrics": m, "sigma": [(x.xx, x.xy) for x in sig]}))
+
+
+def batch_pass(a) -> None:
+    from .batch import BatchPass, BatchSweep
+    w = workloads.WORKLOADS[a.workload]()
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    s = make_settings(w.tau, w.alpha, w.clockwise, w.particle_speed, w.region_size, w.region_extends, w.density,
+                      w.impurity_radius, w.target_cell_population)
+    prec = N.ES_PRECISION_SPLIT if a.precision is None else a.precision
+    with BatchSweep(chunk_iters=a.chunk_iters, precision=prec) as b:
+        gid = b.add_grid(g)
+        b.set_passes([BatchPass(gid, w.dim, w.phi_steps, bool(a.coherent), w.region_size, g.info().cell_size,
+                                a.field, s, list(w.temperatures))])
+        ms = []
+        for _ in range(a.passes):
+            if a.time:
+                import torch
+                stream = torch.cuda.ExternalStream(b.stream_handle())
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                b.enqueue()
+                e1.record(stream)
+                out, m = b.collect()
+                ms.append(round(e0.elapsed_time(e1), 3))
+            else:
+                out, m = b.run()
+    print(json.dumps({"workload": w.name, "field": a.field, "coherent": a.coherent, "orbits": w.orbits_per_pass,
+                      "batch": True, "ms": ms, "metrics": m[0], "sigma": out[0, :len(w.temperatures)].tolist()}))
 
 
 def compare_split(a) -> None:

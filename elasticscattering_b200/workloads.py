@@ -103,4 +103,61 @@ def config3() -> Workload:
                     target_cell_population=25, fields=[40.0], temperatures=[T_ZERO_STANDIN])
 
 
+@dataclass
+class SweepSample:
+    """One impurity sample of a batched sweep: its Grid seed, start grid and density."""
+    index: int
+    seed: int
+    dim: int
+    density: float
+
+
+@dataclass
+class BatchWorkload:
+    """A sweep over samples x fields x temperatures with per-sample start grids and
+    densities (both sectors per (sample, field), as SimulationRunner runs them,
+    src/SimulationRunner.cpp:91-92)."""
+    name: str
+    samples: list
+    fields: list
+    temperatures: list
+    phi_steps: int
+    region_size: float
+    region_extends: float
+    impurity_radius: float
+    target_cell_population: int
+    draw_seed: int
+    particle_speed: float = 1.68e5
+    alpha: float = 0.3
+    tau: float = 1e-12
+    clockwise: bool = True
+
+    @property
+    def orbits(self) -> int:
+        return sum(s.dim * s.dim for s in self.samples) * 4 * self.phi_steps * 2 * len(self.fields)
+
+    @property
+    def sigma_points(self) -> int:
+        """One point = one (sample, field, temperature) with both sectors."""
+        return len(self.samples) * len(self.fields) * len(self.temperatures)
+
+
+def config2(n_samples: int = 64, n_fields: int = 32, dims=(129, 257, 513), phi_steps: int = 129,
+            draw_seed: int = 12345, start_seed: int = 0) -> BatchWorkload:
+    """Batched sweep: 64 samples (Grid seeds of start_seed 0, samples 0-63) x 32 fields
+    uniformly spaced 1-40 T x T in {0, 10, 40} K. Per sample, the start grid is drawn from
+    {129^2, 257^2, 513^2} and the density log-uniformly from 1e15-1e16 m^-2, with a
+    fixed draw seed (12345) so that the instance set is reproducible."""
+    import numpy as np
+    rng = np.random.default_rng(draw_seed)
+    dim_draw = rng.choice(np.asarray(dims), size=n_samples)
+    dens_draw = 10.0 ** rng.uniform(15.0, 16.0, size=n_samples)
+    samples = [SweepSample(k, (start_seed + 100) * (k + 1), int(dim_draw[k]), float(dens_draw[k]))
+               for k in range(n_samples)]
+    fields = [float(b) for b in np.linspace(1.0, 40.0, n_fields)]
+    return BatchWorkload(f"config2-{n_samples}x{n_fields}x3", samples, fields, [0.0, 10.0, 40.0], phi_steps,
+                         region_size=1e-6, region_extends=orbit_diameter(1.68e5, min(fields)),
+                         impurity_radius=2e-9, target_cell_population=12, draw_seed=draw_seed)
+
+
 WORKLOADS = {"config0": config0, "config1": config1, "config3": config3}

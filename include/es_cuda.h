@@ -234,6 +234,80 @@ es_status es_derive_temperatures_noalloc(const double* d_lifetimes, int32_t posi
                                          const double* temperatures, int32_t n_t, double* d_out_sigma,
                                          void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Batched sweeps. No reference counterpart: the reference runs one
+ * (sample, field, sector) pass per Simulation::ComputeSigmas call
+ * (src/SimulationRunner.cpp:103-151). A batch holds many such passes -- each
+ * with its own grid, start-position grid, phase count, field, sector and
+ * temperature list -- and computes all of them in one persistent kernel,
+ * launched from a CUDA graph that is recorded once and replayed; changing the
+ * instance table does not re-record it. Lifetimes are not materialised:
+ * stages (b) and (c) are fused into the lifetime kernel. Results are
+ * bit-reproducible run to run (fixed-point accumulation).
+ * ------------------------------------------------------------------------- */
+
+#define ES_BATCH_MAX_T 8
+
+typedef struct es_batch es_batch;
+
+/* One pass: the arguments of es_create + es_init_sample + es_compute_sigmas
+ * for one (sample, field, sector). */
+typedef struct es_batch_instance {
+    int32_t grid;                   /* index returned by es_batch_add_grid */
+    int32_t positions_per_row;      /* dim, odd, >= 3 */
+    int32_t particles_per_quadrant; /* phi_steps, odd, >= 3 */
+    int32_t coherent;               /* sector */
+    double region_size;
+    double grid_cell_size;          /* GridInformation::cell_size (start offset), as es_sim_desc */
+    double magnetic_field;
+    es_settings settings;           /* tau, alpha, is_clockwise, particle_speed are read */
+    int32_t n_t;                    /* 1..ES_BATCH_MAX_T temperatures, at most 4 distinct tau */
+    double temperatures[ES_BATCH_MAX_T];
+} es_batch_instance;
+
+/* Launch choices of a batch (picked by the autotuner). */
+typedef struct es_batch_tuning {
+    int32_t chunk_iters;    /* orbits per work item = 32 * chunk_iters */
+    int32_t blocks_per_sm;  /* resident blocks of 256 threads per SM: 3 or 4 */
+    int32_t precision;      /* es_precision */
+} es_batch_tuning;
+
+es_status es_batch_create(int32_t device_ordinal, es_batch** out);
+es_status es_batch_destroy(es_batch* b);
+/* Message of the last failure on this batch ("" if none). */
+const char* es_batch_last_error(const es_batch* b);
+es_status es_batch_get_tuning(const es_batch* b, es_batch_tuning* out);
+es_status es_batch_set_tuning(es_batch* b, const es_batch_tuning* t);
+
+/* Copies one impurity grid (same arrays as es_upload_grid) to the device and
+ * returns its index in *out_grid. Grids stay resident until es_batch_clear. */
+es_status es_batch_add_grid(es_batch* b, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
+                            const es_impurity_settings* is, int32_t* out_grid);
+
+/* Releases every grid and instance of the batch. */
+es_status es_batch_clear(es_batch* b);
+
+/* Sets the passes of the batch (validated as es_create / es_init_sample /
+ * es_compute_sigmas validate them). */
+es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int32_t n);
+
+/* Runs every pass and blocks. out_sigma: n * ES_BATCH_MAX_T * 2 doubles,
+ * [instance][temperature][xx, xy], as es_compute_sigmas returns them per pass.
+ * out_metrics (n entries) may be NULL. */
+es_status es_batch_run(es_batch* b, double* out_sigma, es_metrics* out_metrics);
+
+/* es_batch_run in two halves: enqueue the graph on the batch stream (no host
+ * wait), then wait and convert the results. */
+es_status es_batch_enqueue(es_batch* b);
+es_status es_batch_collect(es_batch* b, double* out_sigma, es_metrics* out_metrics);
+
+/* The batch's cudaStream_t, as an opaque pointer (for event timing). */
+void* es_batch_stream(es_batch* b);
+/* Kernel launches issued by this batch (one per graph replay, one per grid copy). */
+int64_t es_batch_launch_count(const es_batch* b);
+/* Orbits per run of the current instance table. */
+int64_t es_batch_total_orbits(const es_batch* b);
+
 /* Measured FP64 FMA throughput of a device (TFLOP/s, 2 FLOP per FMA): the
  * denominator of the lifetime kernel's roofline. No reference counterpart
  * (the reference publishes no device figures). Runs for a few milliseconds. */

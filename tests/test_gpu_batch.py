@@ -1,0 +1,186 @@
+"""Batched sweeps (es_batch_*) against the per-pass path, through the C ABI.
+
+Each batched pass must reproduce what one Simulation::ComputeSigmas call
+returns for it (src/sim/Simulation.h:128): the per-pass FP64 path
+(SimulationCUDA, ES_PRECISION_FP64) is the judge. Bars:
+- ES_PRECISION_FP64 batch: sigma within 1e-9 relative -- the plain path's parity
+  bar; only the summation order and the fixed-point rounding of the work-item
+  sums differ (observed ~1e-11 on sigma_xy, whose terms cancel) -- and identical
+  metrics;
+- ES_PRECISION_SPLIT batch: sigma within 1e-6 relative (FP32 Boltzmann kernel),
+  identical metrics (every lifetime equals the FP64 one);
+- runs are bit-reproducible, independent of the launch shape, and a replayed
+  graph with a new instance table equals a fresh batch.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from elasticscattering_b200 import Grid, SimulationCUDA, make_settings, workloads
+from elasticscattering_b200 import _native as N
+from elasticscattering_b200.simulation import SampleMetrics
+from elasticscattering_b200.batch import BatchPass, BatchSweep, incoherent_temperature
+
+pytestmark = pytest.mark.gpu
+
+FP64_RTOL = 1e-9
+SPLIT_RTOL = 1e-6
+METRIC_KEYS = ("cells_passed", "impurities_tested", "crossings_tested", "particles_inside_impurity",
+               "particles_escaped", "particles_at_bound", "max_cells_passed", "max_impurities_tested")
+
+SPEED, ALPHA, TAU, L, R_IMP = 1.68e5, 0.3, 1e-12, 1e-6, 2e-9
+FIELDS = (1.5, 7.0, 20.0, 40.0)
+TEMPS = (0.0, 10.0, 40.0)
+# (sample index, start positions per row, phases per quadrant, density)
+SAMPLES = ((0, 17, 9, 1e15), (1, 33, 25, 4e15), (2, 65, 9, 1e16))
+
+
+@pytest.fixture(scope="module")
+def sweep_inputs(cuda_device):
+    ext = workloads.orbit_diameter(SPEED, min(FIELDS))
+    grids = {}
+    for k, dim, ppq, dens in SAMPLES:
+        grids[k] = Grid.from_seed((0 + 100) * (k + 1), L, ext, dens, R_IMP, 12)
+    return ext, grids
+
+
+def make_passes(ext, grids, grid_ids, fields=FIELDS):
+    passes = []
+    temps = [incoherent_temperature(t) for t in TEMPS]
+    for k, dim, ppq, dens in SAMPLES:
+        st = make_settings(TAU, ALPHA, True, SPEED, L, ext, dens, R_IMP, 12)
+        for b in fields:
+            for coherent in (True, False):
+                passes.append(BatchPass(grid_ids[k], dim, ppq, coherent, L, grids[k].info().cell_size, b, st,
+                                        list(temps)))
+    return passes
+
+
+def per_pass_reference(grids, passes, device):
+    """sigma [n, T, 2] and metrics of every pass from the per-pass FP64 path
+    (passes built with grid = sample index)."""
+    out = np.zeros((len(passes), len(TEMPS), 2))
+    mets = []
+    sims = {}
+    try:
+        for n, p in enumerate(passes):
+            key = (p.grid, p.coherent)
+            if key not in sims:
+                sims[key] = SimulationCUDA(p.positions_per_row, p.phi_steps, grids[p.grid].info(), device=device,
+                                           precision=N.ES_PRECISION_FP64)
+                sims[key].InitSample(grids[p.grid], p.settings, p.coherent)
+            sm = SampleMetrics()
+            sig = sims[key].ComputeSigmas(p.magnetic_field, p.temperatures, sample_metrics=sm)
+            for t, s in enumerate(sig):
+                out[n, t] = (s.xx, s.xy)
+            mets.append(sm.iteration_metrics[-1])
+    finally:
+        for s in sims.values():
+            s.close()
+    return out, mets
+
+
+def rel_err(a, b):
+    return np.abs(a - b) / np.abs(b)
+
+
+@pytest.fixture(scope="module")
+def reference(sweep_inputs, cuda_device):
+    ext, grids = sweep_inputs
+    passes = make_passes(ext, grids, {k: k for k, *_rest in SAMPLES})
+    return per_pass_reference(grids, passes, cuda_device)
+
+
+def new_batch(grids, device, precision, chunk_iters=8, blocks_per_sm=4):
+    b = BatchSweep(device, chunk_iters=chunk_iters, blocks_per_sm=blocks_per_sm, precision=precision)
+    ids = {k: b.add_grid(grids[k]) for k, *_rest in SAMPLES}
+    return b, ids
+
+
+@pytest.mark.parametrize("precision,rtol", [(N.ES_PRECISION_FP64, FP64_RTOL), (N.ES_PRECISION_SPLIT, SPLIT_RTOL)])
+def test_batch_matches_per_pass(sweep_inputs, reference, cuda_device, precision, rtol):
+    ext, grids = sweep_inputs
+    ref_sigma, ref_mets = reference
+    b, ids = new_batch(grids, cuda_device, precision)
+    try:
+        passes = make_passes(ext, grids, ids)
+        b.set_passes(passes)
+        out, mets = b.run()
+        got = out[:, :len(TEMPS), :]
+        err = rel_err(got, ref_sigma)
+        assert float(err.max()) <= rtol, (precision, float(err.max()), np.unravel_index(err.argmax(), err.shape))
+        for n, (m, r) in enumerate(zip(mets, ref_mets)):
+            for k in METRIC_KEYS:
+                assert m[k] == r[k], (precision, n, k, m[k], r[k])
+        assert out[:, len(TEMPS):, :].max() == 0.0 and out[:, len(TEMPS):, :].min() == 0.0
+    finally:
+        b.close()
+
+
+def test_batch_bit_reproducible_and_shape_independent(sweep_inputs, cuda_device):
+    ext, grids = sweep_inputs
+    b, ids = new_batch(grids, cuda_device, N.ES_PRECISION_SPLIT, chunk_iters=4, blocks_per_sm=4)
+    try:
+        b.set_passes(make_passes(ext, grids, ids))
+        first, m1 = b.run()
+        second, m2 = b.run()
+        assert np.array_equal(first.view(np.int64), second.view(np.int64))
+        assert m1 == m2
+        b.set_tuning(blocks_per_sm=3)
+        third, m3 = b.run()
+        assert np.array_equal(first.view(np.int64), third.view(np.int64))
+        assert m1 == m3
+        # another work-item size regroups the FP64 partial sums: equal to rounding
+        b.set_tuning(chunk_iters=32)
+        fourth, m4 = b.run()
+        assert float(rel_err(fourth[:, :3], first[:, :3]).max()) <= FP64_RTOL
+        assert m1 == m4
+    finally:
+        b.close()
+
+
+def test_batch_graph_replay_with_new_table(sweep_inputs, cuda_device):
+    """The recorded graph is replayed with a rewritten instance table (same capacity)."""
+    ext, grids = sweep_inputs
+    b, ids = new_batch(grids, cuda_device, N.ES_PRECISION_SPLIT)
+    fresh, fids = new_batch(grids, cuda_device, N.ES_PRECISION_SPLIT)
+    try:
+        b.set_passes(make_passes(ext, grids, ids, fields=(1.5, 7.0)))
+        b.run()
+        launches = b.launch_count()
+        b.set_passes(make_passes(ext, grids, ids, fields=(3.0, 33.0)))
+        replayed, mr = b.run()
+        assert b.launch_count() == launches + 1
+        fresh.set_passes(make_passes(ext, grids, fids, fields=(3.0, 33.0)))
+        direct, md = fresh.run()
+        assert np.array_equal(replayed.view(np.int64), direct.view(np.int64))
+        assert mr == md
+    finally:
+        b.close()
+        fresh.close()
+
+
+def test_batch_rejects_bad_instances(sweep_inputs, cuda_device):
+    ext, grids = sweep_inputs
+    b, ids = new_batch(grids, cuda_device, N.ES_PRECISION_SPLIT)
+    try:
+        good = make_passes(ext, grids, ids, fields=(7.0,))
+        bad = [BatchPass(**{**good[1].__dict__, "grid": 99})]
+        with pytest.raises(N.EsError, match="unknown grid"):
+            b.set_passes(bad)
+        many_t = [BatchPass(**{**good[1].__dict__, "temperatures": [1.0, 2.0, 3.0, 4.0, 5.0]})]
+        with pytest.raises(N.EsError, match="distinct relaxation times"):
+            b.set_passes(many_t)
+        far = [BatchPass(**{**good[0].__dict__, "region_size": 1.0})]
+        with pytest.raises(N.EsError, match="outside its grid"):
+            b.set_passes(far)
+        zero_t = [BatchPass(**{**good[1].__dict__, "temperatures": [0.0]})]
+        with pytest.raises(N.EsError, match="needs T > 0"):
+            b.set_passes(zero_t)
+        # the batch is still usable
+        b.set_passes(good)
+        out, _ = b.run()
+        assert np.isfinite(out).all()
+    finally:
+        b.close()
