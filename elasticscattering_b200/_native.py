@@ -61,6 +61,9 @@ class Tuning(C.Structure):
 
 
 ES_BATCH_MAX_T = 8
+ES_BATCH_PASS_NODES = 0
+ES_BATCH_GRID = 1
+ES_BATCH_PERSISTENT = 2
 
 
 class BatchInstance(C.Structure):
@@ -73,7 +76,8 @@ class BatchInstance(C.Structure):
 
 class BatchTuning(C.Structure):
     """es_batch_tuning: launch choices of a batch."""
-    _fields_ = [("chunk_iters", C.c_int32), ("blocks_per_sm", C.c_int32), ("precision", C.c_int32)]
+    _fields_ = [("chunk_iters", C.c_int32), ("blocks_per_sm", C.c_int32), ("precision", C.c_int32),
+                ("mode", C.c_int32)]
 
 
 class SimDesc(C.Structure):

@@ -74,8 +74,8 @@ def sweep_passes(wl, grid_ids: list, grid_cell_sizes: list, samples=None, fields
 class BatchSweep:
     """Owner of one es_batch (device buffers, stream, recorded graph)."""
 
-    def __init__(self, device: int = 0, chunk_iters: int = 8, blocks_per_sm: int = 4,
-                 precision: int = N.ES_PRECISION_SPLIT):
+    def __init__(self, device: int = 0, chunk_iters: int = 32, blocks_per_sm: int = 4,
+                 precision: int = N.ES_PRECISION_SPLIT, mode: int = N.ES_BATCH_PERSISTENT):
         lib = N.cuda_lib()
         h = C.c_void_p()
         st = lib.es_batch_create(int(device), C.byref(h))
@@ -83,7 +83,8 @@ class BatchSweep:
             N.check(st, None)
         self._b = h
         self.passes: list[BatchPass] = []
-        self.set_tuning(chunk_iters=chunk_iters, blocks_per_sm=blocks_per_sm, precision=precision)
+        self.set_tuning(chunk_iters=chunk_iters, blocks_per_sm=blocks_per_sm, precision=precision,
+                        mode=mode)
 
     def close(self) -> None:
         if getattr(self, "_b", None) and self._b.value:
@@ -105,12 +106,12 @@ class BatchSweep:
     def get_tuning(self) -> dict:
         t = N.BatchTuning()
         self._check(N.cuda_lib().es_batch_get_tuning(self._b, C.byref(t)))
-        return {"chunk_iters": t.chunk_iters, "blocks_per_sm": t.blocks_per_sm, "precision": t.precision}
+        return {name: int(getattr(t, name)) for name, _ in N.BatchTuning._fields_}
 
     def set_tuning(self, **fields) -> None:
-        cur = self.get_tuning() if self._b.value and getattr(self, "_tuned", False) else {}
+        cur = self.get_tuning()
         cur.update(fields)
-        t = N.BatchTuning(int(cur["chunk_iters"]), int(cur["blocks_per_sm"]), int(cur["precision"]))
+        t = N.BatchTuning(*[int(cur[name]) for name, _ in N.BatchTuning._fields_])
         self._check(N.cuda_lib().es_batch_set_tuning(self._b, C.byref(t)))
         self._tuned = True
 

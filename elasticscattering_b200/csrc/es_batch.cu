@@ -73,7 +73,13 @@ struct BatchLaunch {
     unsigned long long* counter;      // work-item counter, zeroed before each run
     int* error;
     int chunk_iters;
+    // split precision: orbits for the FP64 re-trace, as (pass << 40) | orbit
+    unsigned long long* retrace;
+    unsigned long long* retrace_count;
+    long long retrace_cap;
 };
+
+constexpr int kRetraceOrbitBits = 40;   // orbit index bits of a re-trace entry (passes < 2^40 orbits)
 
 namespace {
 
@@ -91,42 +97,76 @@ __device__ __forceinline__ double simpson_w(int i, int dim)
     return (i == 0 || i == dim - 1) ? 1.0 : main_multiplier;
 }
 
-// x mod 2 pi into [-pi, pi], in FP64.
-__device__ __forceinline__ double reduce_2pi(double x)
+// sin and cos of an FP64 angle, evaluated in FP32. The quadrant reduction
+// x = q pi/2 + r, |r| <= pi/4, is done in FP64 (exact enough for any |x| the
+// kernel meets, a few thousand radians at most); sin r and cos r are their
+// Taylor polynomials (degree 9 and 10: truncation below 2e-9 on |r| <= pi/4),
+// evaluated by Horner's rule in FP32. Measured against FP64 sin/cos over
+// [-50, 50] and down to |x| = 1e-12: at most 1.5 ulp. The code is short and
+// branch-free, which matters in a kernel limited by instruction fetch.
+__device__ __forceinline__ void sincos_reduced(double x, float& s_out, float& c_out)
 {
-    constexpr double kTwoPi = 6.283185307179586476925;
-    return x - kTwoPi * rint(x * (1.0 / kTwoPi));
+    constexpr double kTwoOverPi = 0.636619772367581343076;
+    constexpr double kHalfPi = 1.570796326794896619231;
+    const double q = rint(x * kTwoOverPi);
+    const float r = (float)(x - q * kHalfPi);
+    const float r2 = r * r;
+    const float s = r + r * r2 * (-1.0f / 6.0f + r2 * (1.0f / 120.0f + r2 * (-1.0f / 5040.0f + r2 * (1.0f / 362880.0f))));
+    const float c = 1.0f + r2 * (-0.5f + r2 * (1.0f / 24.0f + r2 * (-1.0f / 720.0f + r2 * (1.0f / 40320.0f +
+                                                                                             r2 * (-1.0f / 3628800.0f)))));
+    const int n = ((int)(long long)q) & 3;
+    s_out = (n == 0) ? s : (n == 1) ? c : (n == 2) ? -s : -c;
+    c_out = (n == 0) ? c : (n == 1) ? -s : (n == 2) ? -c : s;
+}
+
+// 1 - exp(-x) for x >= 0 in FP32: the Taylor series (degree 8, nested) below
+// 0.5, where 1 - exp(-x) would cancel; 1 - expf(-x) above. Relative error
+// below 2e-7 on [1e-10, 15].
+__device__ __forceinline__ float one_minus_exp_neg(float x)
+{
+    if (x < 0.5f)
+        return x * (1.0f - x * 0.5f * (1.0f - x * (1.0f / 3.0f) * (1.0f - x * 0.25f * (1.0f - x * 0.2f *
+               (1.0f - x * (1.0f / 6.0f) * (1.0f - x * (1.0f / 7.0f) * (1.0f - x * 0.125f)))))));
+    return 1.0f - expf(-x);
 }
 
 // GetSigma (src/sim/es/util.h:34-46) for the truncated lifetimes of one orbit,
-// FP32. With z = exp(-t/tau), e1 = 1 - z = -expm1(-t/tau), h = w t / 2:
+// FP32. With z = exp(-t/tau), e1 = 1 - z, h = w t / 2:
 //   cos(phi) - z cos(phi + 2h)       = cos(phi) e1 + 2 z sin(h) sin(phi + h)
 //   w tau (z sin(phi + 2h) - sin(phi)) = w tau (2 z sin(h) cos(phi + h) - e1 sin(phi))
 // Both right-hand sides are sums of products of well-conditioned factors, so
 // each orbit's value keeps FP32 relative accuracy even for t << tau, where
 // the left-hand sides cancel (there FP32 loses up to 1e-5 of sigma_xy). The
 // angles h and phi + h are formed and reduced in FP64.
+__device__ __forceinline__ void kernel_fp32(const BatchInstanceD& I, int k, double raw, const PhaseSigma& ph,
+                                            float& r_xx, float& r_xy)
+{
+    const float c = (float)ph.cos_phi, s = (float)ph.sin_phi;
+    const double max_lt = I.max_lt[k];
+    const double lt = raw < max_lt ? raw : max_lt;
+    const float e1 = one_minus_exp_neg((float)(lt * I.inv_tau[k]));
+    const float z = 1.0f - e1;
+    const double h = 0.5 * I.w_signed * lt;
+    float sh, ch, sp, cp;
+    sincos_reduced(h, sh, ch);
+    sincos_reduced(ph.phi + h, sp, cp);
+    const float zs = 2.0f * z * sh;
+    const float wt = (float)I.wtau[k];
+    const float r = c * e1 + zs * sp + wt * (zs * cp - e1 * s);
+    r_xx = r * c;
+    r_xy = r * s;
+}
+
 __device__ __forceinline__ void add_kernel_fp32(const BatchInstanceD& I, double raw, const PhaseSigma& ph,
                                                 double wgt, double* slots)
 {
-    const float c = (float)ph.cos_phi, s = (float)ph.sin_phi;
-#pragma unroll
-    for (int k = 0; k < kBatchMaxTau; k++) {
-        if (k < I.n_tau) {
-            const double lt = raw < I.max_lt[k] ? raw : I.max_lt[k];
-            const float x = (float)(lt * I.inv_tau[k]);
-            const float e1 = -expm1f(-x);
-            const float z = 1.0f - e1;
-            const double h = 0.5 * I.w_signed * lt;
-            const float sh = sinf((float)reduce_2pi(h));
-            float sp, cp;
-            sincosf((float)reduce_2pi(ph.phi + h), &sp, &cp);
-            const float zs = 2.0f * z * sh;
-            const float wt = (float)I.wtau[k];
-            const float r = c * e1 + zs * sp + wt * (zs * cp - e1 * s);
-            slots[(2 * k) * 32] += wgt * (double)(r * c);
-            slots[(2 * k + 1) * 32] += wgt * (double)(r * s);
-        }
+    const int n_tau = I.n_tau;
+#pragma unroll 1
+    for (int k = 0; k < n_tau; k++) {
+        float r_xx, r_xy;
+        kernel_fp32(I, k, raw, ph, r_xx, r_xy);
+        slots[(2 * k) * 32] += wgt * (double)r_xx;
+        slots[(2 * k + 1) * 32] += wgt * (double)r_xy;
     }
 }
 
@@ -136,25 +176,23 @@ __device__ __forceinline__ void add_kernel_fp64(const BatchInstanceD& I, double 
 {
     double sa_raw, ca_raw;
     sincos(ph.phi + I.w_signed * raw, &sa_raw, &ca_raw);
-#pragma unroll
-    for (int k = 0; k < kBatchMaxTau; k++) {
-        if (k < I.n_tau) {
-            const bool keep = raw < I.max_lt[k];
-            const double lt = keep ? raw : I.max_lt[k];
-            double sa = sa_raw, ca = ca_raw;
-            if (!keep) sincos(ph.phi + I.w_signed * lt, &sa, &ca);
-            const double z = exp(-lt / I.tau[k]);
-            double r = ph.cos_phi - ca * z;
-            r += I.wtau[k] * sa * z;
-            r -= I.wtau[k] * ph.sin_phi;
-            slots[(2 * k) * 32] += ((r * ph.cos_phi) * ph.weight) * wpos;
-            slots[(2 * k + 1) * 32] += ((r * ph.sin_phi) * ph.weight) * wpos;
-        }
+#pragma unroll 1
+    for (int k = 0; k < I.n_tau; k++) {
+        const bool keep = raw < I.max_lt[k];
+        const double lt = keep ? raw : I.max_lt[k];
+        double sa = sa_raw, ca = ca_raw;
+        if (!keep) sincos(ph.phi + I.w_signed * lt, &sa, &ca);
+        const double z = exp(-lt / I.tau[k]);
+        double r = ph.cos_phi - ca * z;
+        r += I.wtau[k] * sa * z;
+        r -= I.wtau[k] * ph.sin_phi;
+        slots[(2 * k) * 32] += ((r * ph.cos_phi) * ph.weight) * wpos;
+        slots[(2 * k + 1) * 32] += ((r * ph.sin_phi) * ph.weight) * wpos;
     }
 }
 
-// Plain FP64 TraceOrbit of orbit g (start cell checked by the caller).
-__device__ __noinline__ double fp64_lifetime(const LifetimeLaunch& P, long long g, OrbitCounters* cnt, int* flags)
+// Plain FP64 TraceOrbit of orbit g, with the start-cell check.
+__device__ __forceinline__ double fp64_lifetime(const LifetimeLaunch& P, long long g, OrbitCounters* cnt, int* flags)
 {
     GridD gr;
     gr.imps = P.imps;
@@ -226,33 +264,48 @@ __global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks) batch_kernel(Bat
             const long long g = g0 + (long long)it * 32 + lane;
             const bool active = g < I.L.n_orbits;
             if (!__any_sync(0xffffffffu, active)) break;
-            unsigned cells = 0, imps = 0, cross = 0, starts = 0, retraced = 0;
+            unsigned cells = 0, imps = 0, cross = 0, starts = 0;
             int flags = kTraceOk;
+            bool retrace = false;
             if (active) {
                 double lt = 0.0;
                 if (kPrec == ES_PRECISION_SPLIT) {
                     SplitCounters sc;
-                    if (split_orbit(I.L, g, sc, flags, lt)) {
-                        OrbitCounters oc;
-                        lt = fp64_lifetime(I.L, g, &oc, &flags);
-                        cells = oc.cells, imps = oc.imps, cross = oc.crossings, starts = oc.start_tests;
-                        retraced = 1;
-                    } else {
-                        cells = sc.cells, imps = sc.imps, cross = sc.crossings, starts = sc.start_tests;
-                    }
+                    retrace = split_orbit(SharedFields{&I.L}, g, sc, flags, lt);
+                    cells = sc.cells, imps = sc.imps, cross = sc.crossings, starts = sc.start_tests;
                 } else {
                     OrbitCounters oc;
                     lt = fp64_lifetime(I.L, g, &oc, &flags);
                     cells = oc.cells, imps = oc.imps, cross = oc.crossings, starts = oc.start_tests;
                 }
-                const int v = (int)(g % I.L.n_phase);
-                const long long pidx = g / I.L.n_phase;
-                const int i = (int)(pidx % I.L.dim);
-                const int j = (int)(pidx / I.L.dim);
-                const double wpos = simpson_w(j, I.L.dim) * simpson_w(i, I.L.dim);
-                const PhaseSigma ph = I.phase_sigma[v];
-                if (kPrec == ES_PRECISION_SPLIT) add_kernel_fp32(I, lt, ph, wpos * ph.weight, slots);
-                else add_kernel_fp64(I, lt, ph, wpos, slots);
+                if (!retrace) {
+                    const int n_phase = I.L.n_phase, dim = I.L.dim;
+                    const int v = (int)(g % n_phase);
+                    const long long pidx = g / n_phase;
+                    const int i = (int)(pidx % dim);
+                    const int j = (int)(pidx / dim);
+                    const double wpos = simpson_w(j, dim) * simpson_w(i, dim);
+                    const PhaseSigma ph = I.phase_sigma[v];
+                    if (kPrec == ES_PRECISION_SPLIT) add_kernel_fp32(I, lt, ph, wpos * ph.weight, slots);
+                    else add_kernel_fp64(I, lt, ph, wpos, slots);
+                }
+            }
+            if (kPrec == ES_PRECISION_SPLIT) {
+                // uncertain orbits go to the FP64 re-trace list (one atomic per warp);
+                // the re-trace kernel counts and integrates them
+                const unsigned want = __ballot_sync(0xffffffffu, retrace);
+                if (want) {
+                    unsigned long long base = 0;
+                    if (lane == 0) base = atomicAdd(B.retrace_count, (unsigned long long)__popc(want));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (retrace) {
+                        const unsigned long long slot = base + __popc(want & ((1u << lane) - 1u));
+                        if (slot < (unsigned long long)B.retrace_cap)
+                            B.retrace[slot] = ((unsigned long long)cur << kRetraceOrbitBits) | (unsigned long long)g;
+                        else
+                            atomicOr(B.error, kErrRetraceOverflow);
+                    }
+                }
             }
             const unsigned s_cells = __reduce_add_sync(0xffffffffu, cells);
             const unsigned s_imps = __reduce_add_sync(0xffffffffu, imps);
@@ -261,7 +314,6 @@ __global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks) batch_kernel(Bat
             const unsigned s_inside = __reduce_add_sync(0xffffffffu, (flags & kTraceInside) ? 1u : 0u);
             const unsigned s_escaped = __reduce_add_sync(0xffffffffu, (flags & kTraceEscaped) ? 1u : 0u);
             const unsigned s_bound = __reduce_add_sync(0xffffffffu, (flags & kTraceAtBound) ? 1u : 0u);
-            const unsigned s_retraced = __reduce_add_sync(0xffffffffu, retraced);
             const unsigned m_cells = __reduce_max_sync(0xffffffffu, cells);
             const unsigned m_imps = __reduce_max_sync(0xffffffffu, imps);
             if (lane == 0) {
@@ -272,7 +324,6 @@ __global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks) batch_kernel(Bat
                 met[kMetInside] += s_inside;
                 met[kMetEscaped] += s_escaped;
                 met[kMetAtBound] += s_bound;
-                met[kMetRetraced] += s_retraced;
                 met[kMetMaxCells] = max(met[kMetMaxCells], (unsigned long long)m_cells);
                 met[kMetMaxImps] = max(met[kMetMaxImps], (unsigned long long)m_imps);
             }
@@ -300,21 +351,306 @@ __global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks) batch_kernel(Bat
     }
 }
 
-template <int kPrec, int kMinBlocks>
-cudaError_t launch_batch_t(const BatchLaunch& B, int n_sm, cudaStream_t s)
+// One block = one work item of 256 consecutive orbits of one pass (one orbit
+// per thread): a thread holds no loop state across its walk, as in the
+// single-pass kernels. The block ends with a fixed-order reduction and one
+// fixed-point atomic per sum. I is the pass record and f reads the walk's
+// constants from it (kernel parameter or shared memory).
+template <int kPrec, class F>
+__device__ __forceinline__ void block_item(const BatchInstanceD& I, const F& f, const BatchLaunch& B, long long pass,
+                                           long long item_in_pass)
 {
-    batch_kernel<kPrec, kMinBlocks><<<n_sm * kMinBlocks, kBatchWarps * 32, 0, s>>>(B);
+    __shared__ double s_sum[kBatchWarps][2 * kBatchMaxTau];
+    __shared__ unsigned s_met[kBatchWarps][kMetCount];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    const long long g = item_in_pass * (kBatchWarps * 32) + threadIdx.x;
+    const bool active = g < I.L.n_orbits;
+    unsigned cells = 0, imps = 0, cross = 0, starts = 0;
+    int flags = kTraceOk;
+    bool retrace = false;
+    double lt = 0.0;
+    if (active) {
+        if (kPrec == ES_PRECISION_SPLIT) {
+            SplitCounters sc;
+            retrace = split_orbit(f, g, sc, flags, lt);
+            cells = sc.cells, imps = sc.imps, cross = sc.crossings, starts = sc.start_tests;
+        } else {
+            OrbitCounters oc;
+            lt = fp64_lifetime(I.L, g, &oc, &flags);
+            cells = oc.cells, imps = oc.imps, cross = oc.crossings, starts = oc.start_tests;
+        }
+    }
+
+    // this orbit's Simpson-weighted kernel values, per relaxation time
+    double val[2 * kBatchMaxTau];
+#pragma unroll
+    for (int k = 0; k < 2 * kBatchMaxTau; k++) val[k] = 0.0;
+    if (active && !retrace) {
+        const int n_phase = I.L.n_phase, dim = I.L.dim;
+        const int v = (int)(g % n_phase);
+        const long long pidx = g / n_phase;
+        const int i = (int)(pidx % dim);
+        const int j = (int)(pidx / dim);
+        const double wpos = simpson_w(j, dim) * simpson_w(i, dim);
+        const PhaseSigma ph = I.phase_sigma[v];
+        if (kPrec == ES_PRECISION_SPLIT) {
+            const double wgt = wpos * ph.weight;
+#pragma unroll
+            for (int k = 0; k < kBatchMaxTau; k++) {
+                if (k < I.n_tau) {
+                    float r_xx, r_xy;
+                    kernel_fp32(I, k, lt, ph, r_xx, r_xy);
+                    val[2 * k] = wgt * (double)r_xx;
+                    val[2 * k + 1] = wgt * (double)r_xy;
+                }
+            }
+        } else {
+            double sa_raw, ca_raw;
+            sincos(ph.phi + I.w_signed * lt, &sa_raw, &ca_raw);
+#pragma unroll
+            for (int k = 0; k < kBatchMaxTau; k++) {
+                if (k < I.n_tau) {
+                    const bool keep = lt < I.max_lt[k];
+                    const double t = keep ? lt : I.max_lt[k];
+                    double sa = sa_raw, ca = ca_raw;
+                    if (!keep) sincos(ph.phi + I.w_signed * t, &sa, &ca);
+                    const double z = exp(-t / I.tau[k]);
+                    double r = ph.cos_phi - ca * z;
+                    r += I.wtau[k] * sa * z;
+                    r -= I.wtau[k] * ph.sin_phi;
+                    val[2 * k] = ((r * ph.cos_phi) * ph.weight) * wpos;
+                    val[2 * k + 1] = ((r * ph.sin_phi) * ph.weight) * wpos;
+                }
+            }
+        }
+    }
+    if (kPrec == ES_PRECISION_SPLIT) {
+        const unsigned want = __ballot_sync(0xffffffffu, retrace);
+        if (want) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(B.retrace_count, (unsigned long long)__popc(want));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (retrace) {
+                const unsigned long long slot = base + __popc(want & ((1u << lane) - 1u));
+                if (slot < (unsigned long long)B.retrace_cap)
+                    B.retrace[slot] = ((unsigned long long)pass << kRetraceOrbitBits) | (unsigned long long)g;
+                else
+                    atomicOr(B.error, kErrRetraceOverflow);
+            }
+        }
+    }
+
+    // block reduction: fixed shuffle tree per warp, then warps in order
+#pragma unroll
+    for (int k = 0; k < 2 * kBatchMaxTau; k++) {
+        if (k < 2 * I.n_tau) {
+            const double s = warp_sum_d(val[k]);
+            if (lane == 0) s_sum[warp][k] = s;
+        }
+    }
+    {
+        const unsigned m[kMetCount] = {
+            __reduce_add_sync(0xffffffffu, cells),
+            __reduce_add_sync(0xffffffffu, imps),
+            __reduce_add_sync(0xffffffffu, (flags & kTraceInside) ? 1u : 0u),
+            __reduce_add_sync(0xffffffffu, (flags & kTraceEscaped) ? 1u : 0u),
+            __reduce_add_sync(0xffffffffu, (flags & kTraceAtBound) ? 1u : 0u),
+            __reduce_max_sync(0xffffffffu, imps),
+            __reduce_max_sync(0xffffffffu, cells),
+            __reduce_add_sync(0xffffffffu, cross),
+            __reduce_add_sync(0xffffffffu, starts),
+            0u};
+        static_assert(kMetCells == 0 && kMetImps == 1 && kMetInside == 2 && kMetEscaped == 3 && kMetAtBound == 4 &&
+                          kMetMaxImps == 5 && kMetMaxCells == 6 && kMetCrossings == 7 && kMetStartTests == 8 &&
+                          kMetRetraced == 9 && kMetCount == 10,
+                      "metric slot order");
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < kMetCount; k++) s_met[warp][k] = m[k];
+        }
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < 2 * I.n_tau) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kBatchWarps; w++) s += s_sum[w][t];
+        const long long q = __double2ll_rn(s * I.fx_scale);
+        if (q != 0) atomicAdd(I.acc + t, (unsigned long long)q);
+    } else if (t >= 32 && t < 32 + kMetCount) {
+        const int k = t - 32;
+        unsigned long long s = 0;
+        const bool is_max = (k == kMetMaxCells || k == kMetMaxImps);
+#pragma unroll
+        for (int w = 0; w < kBatchWarps; w++)
+            s = is_max ? max(s, (unsigned long long)s_met[w][k]) : s + s_met[w][k];
+        if (s != 0) {
+            if (is_max) atomicMax(I.metrics + k, s);
+            else atomicAdd(I.metrics + k, s);
+        }
+    }
+}
+
+// Block-per-item over the whole batch in one launch: each block finds its
+// pass by binary search and stages the pass record in shared memory.
+template <int kPrec, int kMinBlocks>
+__global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks) batch_grid_kernel(BatchLaunch B)
+{
+    __shared__ BatchInstanceD s_inst;
+    __shared__ long long s_pass;
+    const long long item = blockIdx.x;
+    if (threadIdx.x == 0) {
+        long long lo = 0, hi = *B.n_inst - 1;
+        while (lo < hi) {
+            const long long mid = (lo + hi + 1) >> 1;
+            if (B.chunk_begin[mid] <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        s_pass = lo;
+    }
+    __syncthreads();
+    const long long pass = s_pass;
+    {
+        const int4* src = reinterpret_cast<const int4*>(B.inst + pass);
+        int4* dst = reinterpret_cast<int4*>(&s_inst);
+        for (int k = threadIdx.x; k < (int)(sizeof(BatchInstanceD) / 16); k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    block_item<kPrec>(s_inst, SharedFields{&s_inst.L}, B, pass, item - s_inst.chunk_begin);
+}
+
+// Block-per-item over one pass, whose record is the kernel parameter: the
+// walk's constants are constant-bank operands, as in the single-pass kernels.
+// The batch graph holds one such kernel node per pass, on parallel branches.
+template <int kPrec, int kMinBlocks>
+__global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks)
+    batch_pass_kernel(BatchLaunch B, BatchInstanceD I, long long pass)
+{
+    block_item<kPrec>(I, LaunchFields{I.L}, B, pass, blockIdx.x);
+}
+
+// The listed orbits of a split run, in FP64 (TraceOrbit, src/sim/es/lifetime.h:78-148),
+// then integrated like every other orbit. Each warp takes a contiguous slice of
+// the list (entries are appended in roughly pass order), its lanes accumulate
+// fixed-point sums and metrics per pass and add them when the pass changes.
+__global__ void __launch_bounds__(256, 2) batch_retrace_kernel(BatchLaunch B)
+{
+    const unsigned long long n = min(*B.retrace_count, (unsigned long long)B.retrace_cap);
+    const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x / 32);
+    const unsigned long long wid = (unsigned long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const unsigned long long per = (n + warps - 1) / warps;
+    const unsigned long long e_begin = wid * per;
+    const unsigned long long e_end = min(n, e_begin + per);
+    constexpr unsigned long long kOrbitMask = (1ull << kRetraceOrbitBits) - 1ull;
+
+    long long cur = -1;
+    long long acc[2 * kBatchMaxTau];
+    unsigned long long m_sum[8], m_cells = 0, m_imps = 0;
+    auto flush = [&]() {
+        if (cur < 0) return;
+        const BatchInstanceD& I = B.inst[cur];
+#pragma unroll
+        for (int k = 0; k < 2 * kBatchMaxTau; k++)
+            if (acc[k] != 0) atomicAdd(I.acc + k, (unsigned long long)acc[k]);
+        const int slot[8] = {kMetCells, kMetImps, kMetCrossings, kMetStartTests, kMetInside, kMetEscaped, kMetAtBound,
+                             kMetRetraced};
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (m_sum[k] != 0) atomicAdd(I.metrics + slot[k], m_sum[k]);
+        if (m_cells) atomicMax(I.metrics + kMetMaxCells, m_cells);
+        if (m_imps) atomicMax(I.metrics + kMetMaxImps, m_imps);
+    };
+    for (unsigned long long e = e_begin + lane; e < e_end; e += 32) {
+        const unsigned long long ent = B.retrace[e];
+        const long long inst = (long long)(ent >> kRetraceOrbitBits);
+        const long long g = (long long)(ent & kOrbitMask);
+        if (inst != cur) {
+            flush();
+            cur = inst;
+#pragma unroll
+            for (int k = 0; k < 2 * kBatchMaxTau; k++) acc[k] = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) m_sum[k] = 0;
+            m_cells = m_imps = 0;
+        }
+        const BatchInstanceD& I = B.inst[inst];
+        OrbitCounters oc;
+        int flags = kTraceOk;
+        const double lt = fp64_lifetime(I.L, g, &oc, &flags);
+        const int v = (int)(g % I.L.n_phase);
+        const long long pidx = g / I.L.n_phase;
+        const int i = (int)(pidx % I.L.dim);
+        const int j = (int)(pidx / I.L.dim);
+        const PhaseSigma ph = I.phase_sigma[v];
+        const double wgt = simpson_w(j, I.L.dim) * simpson_w(i, I.L.dim) * ph.weight;
+#pragma unroll
+        for (int k = 0; k < kBatchMaxTau; k++) {
+            if (k < I.n_tau) {
+                float r_xx, r_xy;
+                kernel_fp32(I, k, lt, ph, r_xx, r_xy);
+                acc[2 * k] += __double2ll_rn(wgt * (double)r_xx * I.fx_scale);
+                acc[2 * k + 1] += __double2ll_rn(wgt * (double)r_xy * I.fx_scale);
+            }
+        }
+        m_sum[0] += (unsigned)oc.cells;
+        m_sum[1] += (unsigned)oc.imps;
+        m_sum[2] += (unsigned)oc.crossings;
+        m_sum[3] += (unsigned)oc.start_tests;
+        m_sum[4] += (flags & kTraceInside) ? 1u : 0u;
+        m_sum[5] += (flags & kTraceEscaped) ? 1u : 0u;
+        m_sum[6] += (flags & kTraceAtBound) ? 1u : 0u;
+        m_sum[7] += 1u;
+        m_cells = max(m_cells, (unsigned long long)oc.cells);
+        m_imps = max(m_imps, (unsigned long long)oc.imps);
+    }
+    flush();
+}
+
+template <int kPrec, int kMinBlocks>
+cudaError_t launch_batch_t(const BatchLaunch& B, int mode, int n_sm, long long n_items, cudaStream_t s)
+{
+    if (mode == ES_BATCH_PERSISTENT) batch_kernel<kPrec, kMinBlocks><<<n_sm * kMinBlocks, kBatchWarps * 32, 0, s>>>(B);
+    else batch_grid_kernel<kPrec, kMinBlocks><<<(unsigned)n_items, kBatchWarps * 32, 0, s>>>(B);
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch(const BatchLaunch& B, int precision, int blocks_per_sm, int n_sm, cudaStream_t s)
+template <int kPrec, int kMinBlocks>
+cudaError_t launch_pass_t(const BatchLaunch& B, const BatchInstanceD& I, long long pass, long long n_items,
+                          cudaStream_t s)
 {
-    if (precision == ES_PRECISION_SPLIT) {
-        if (blocks_per_sm == 3) return launch_batch_t<ES_PRECISION_SPLIT, 3>(B, n_sm, s);
-        return launch_batch_t<ES_PRECISION_SPLIT, 4>(B, n_sm, s);
-    }
-    if (blocks_per_sm == 3) return launch_batch_t<ES_PRECISION_FP64, 3>(B, n_sm, s);
-    return launch_batch_t<ES_PRECISION_FP64, 4>(B, n_sm, s);
+    batch_pass_kernel<kPrec, kMinBlocks><<<(unsigned)n_items, kBatchWarps * 32, 0, s>>>(B, I, pass);
+    return cudaGetLastError();
+}
+
+// ES_BATCH_GRID / ES_BATCH_PERSISTENT: the one kernel over every pass.
+cudaError_t launch_batch(const BatchLaunch& B, int precision, int blocks_per_sm, int mode, int n_sm,
+                         long long n_items, cudaStream_t s)
+{
+    if (precision == ES_PRECISION_SPLIT)
+        return (blocks_per_sm == 3) ? launch_batch_t<ES_PRECISION_SPLIT, 3>(B, mode, n_sm, n_items, s)
+                                    : launch_batch_t<ES_PRECISION_SPLIT, 4>(B, mode, n_sm, n_items, s);
+    return (blocks_per_sm == 3) ? launch_batch_t<ES_PRECISION_FP64, 3>(B, mode, n_sm, n_items, s)
+                                : launch_batch_t<ES_PRECISION_FP64, 4>(B, mode, n_sm, n_items, s);
+}
+
+// ES_BATCH_PASS_NODES: the kernel of one pass.
+cudaError_t launch_pass(const BatchLaunch& B, const BatchInstanceD& I, long long pass, long long n_items,
+                        int precision, int blocks_per_sm, cudaStream_t s)
+{
+    if (precision == ES_PRECISION_SPLIT)
+        return (blocks_per_sm == 3) ? launch_pass_t<ES_PRECISION_SPLIT, 3>(B, I, pass, n_items, s)
+                                    : launch_pass_t<ES_PRECISION_SPLIT, 4>(B, I, pass, n_items, s);
+    return (blocks_per_sm == 3) ? launch_pass_t<ES_PRECISION_FP64, 3>(B, I, pass, n_items, s)
+                                : launch_pass_t<ES_PRECISION_FP64, 4>(B, I, pass, n_items, s);
+}
+
+// Split precision: the FP64 re-trace of the run's list.
+cudaError_t launch_retrace(const BatchLaunch& B, int n_sm, cudaStream_t s)
+{
+    batch_retrace_kernel<<<n_sm * 2, 256, 0, s>>>(B);
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -343,7 +679,14 @@ struct es_batch {
     cudaStream_t stream = nullptr;
     char err[512] = "";
     int64_t launches = 0;
-    es_batch_tuning tuning{8, 4, ES_PRECISION_SPLIT};
+    // measured best on B200 for config-1-sized passes (the autotuner may choose otherwise)
+    es_batch_tuning tuning{32, 4, ES_PRECISION_SPLIT, ES_BATCH_PERSISTENT};
+    int64_t captured_items = -1;              // grid size recorded in the graph (ES_BATCH_GRID)
+    static constexpr int kBranches = 8;       // parallel graph branches (ES_BATCH_PASS_NODES)
+    cudaStream_t branch[kBranches] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kBranches] = {};
+    std::vector<long long> pass_items;        // work items per pass, kernel order
 
     std::vector<es_batch_grid> grids;
     std::map<std::tuple<int, int, double, double, int>, es_batch_phase> phases;  // (ppq, coherent, alpha, speed, cw)
@@ -369,6 +712,12 @@ struct es_batch {
     unsigned long long* d_counter = nullptr;
     int* d_error = nullptr;
     int* h_error = nullptr;                   // pinned
+    // split precision: FP64 re-trace list (one 8-byte entry per uncertain orbit)
+    unsigned long long* d_retrace = nullptr;
+    long long retrace_cap = 0;
+    unsigned long long* d_retrace_count = nullptr;
+    unsigned long long* h_retrace_count = nullptr;  // pinned
+    int64_t retrace_regrows = 0;
 
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -456,8 +805,38 @@ es_status ensure_capacity(es_batch* b, int64_t n)
     return ES_OK;
 }
 
+// Re-trace list of at least `want` entries (the graph records its address).
+es_status ensure_retrace(es_batch* b, long long want)
+{
+    if (want <= b->retrace_cap) return ES_OK;
+    drop_graph(b);
+    cudaFree(b->d_retrace);
+    b->d_retrace = nullptr;
+    b->retrace_cap = 0;
+    ES_BCUDA(cudaMalloc(&b->d_retrace, sizeof(unsigned long long) * (size_t)want), "re-trace list");
+    b->retrace_cap = want;
+    return ES_OK;
+}
+
+// ES_BATCH_PASS_NODES: one kernel per pass, spread round-robin over the
+// branches forked from the capture stream, joined before the re-trace.
+cudaError_t record_pass_nodes(es_batch* b, const es::BatchLaunch& L)
+{
+    cudaError_t e = cudaEventRecord(b->fork, b->stream);
+    for (int k = 0; e == cudaSuccess && k < es_batch::kBranches; k++) e = cudaStreamWaitEvent(b->branch[k], b->fork, 0);
+    const es::BatchInstanceD* hi = reinterpret_cast<const es::BatchInstanceD*>(b->h_table + b->inst_offset);
+    for (size_t pos = 0; e == cudaSuccess && pos < b->pass_items.size(); pos++)
+        e = es::launch_pass(L, hi[pos], (long long)pos, b->pass_items[pos], b->tuning.precision,
+                            b->tuning.blocks_per_sm, b->branch[pos % es_batch::kBranches]);
+    for (int k = 0; e == cudaSuccess && k < es_batch::kBranches; k++) {
+        e = cudaEventRecord(b->join[k], b->branch[k]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[k], 0);
+    }
+    return e;
+}
+
 // Records the run sequence on the batch stream: table upload, clears, the
-// persistent kernel, readbacks.
+// pass kernels, the FP64 re-trace, readbacks.
 es_status capture(es_batch* b)
 {
     drop_graph(b);
@@ -469,6 +848,9 @@ es_status capture(es_batch* b)
     L.counter = b->d_counter;
     L.error = b->d_error;
     L.chunk_iters = b->tuning.chunk_iters;
+    L.retrace = b->d_retrace;
+    L.retrace_count = b->d_retrace_count;
+    L.retrace_cap = b->retrace_cap;
     const size_t acc_bytes = sizeof(unsigned long long) * 2 * es::kBatchMaxTau * cap;
     const size_t met_bytes = sizeof(unsigned long long) * es::kMetCount * cap;
 
@@ -477,11 +859,20 @@ es_status capture(es_batch* b)
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_acc, 0, acc_bytes, b->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_metrics, 0, met_bytes, b->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), b->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_retrace_count, 0, sizeof(unsigned long long), b->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_error, 0, sizeof(int), b->stream);
-    if (e == cudaSuccess) e = es::launch_batch(L, b->tuning.precision, b->tuning.blocks_per_sm, b->n_sm, b->stream);
+    if (e == cudaSuccess) {
+        if (b->tuning.mode == ES_BATCH_PASS_NODES) e = record_pass_nodes(b, L);
+        else e = es::launch_batch(L, b->tuning.precision, b->tuning.blocks_per_sm, b->tuning.mode, b->n_sm,
+                                  b->total_items, b->stream);
+    }
+    if (e == cudaSuccess && b->tuning.precision == ES_PRECISION_SPLIT) e = es::launch_retrace(L, b->n_sm, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_acc, b->d_acc, acc_bytes, cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_metrics, b->d_metrics, met_bytes, cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_error, b->d_error, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_retrace_count, b->d_retrace_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            b->stream);
     cudaGraph_t g = nullptr;
     const cudaError_t e_end = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess) {
@@ -492,6 +883,7 @@ es_status capture(es_batch* b)
     b->graph = g;
     ES_BCUDA(cudaGraphInstantiate(&b->exec, b->graph, 0), "batch graph instantiation");
     b->graph_dirty = false;
+    b->captured_items = b->total_items;
     return ES_OK;
 }
 
@@ -544,6 +936,17 @@ es_status es_batch_create(int32_t device_ordinal, es_batch** out)
     if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_error, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_error, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_retrace_count, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_retrace_count, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int k = 0; e == cudaSuccess && k < es_batch::kBranches; k++) {
+        e = cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) {
+        *b->h_error = 0;
+        *b->h_retrace_count = 0;
+    }
     if (e != cudaSuccess) {
         char msg[256];
         snprintf(msg, sizeof msg, "es_batch_create: %s", cudaGetErrorString(e));
@@ -565,7 +968,15 @@ es_status es_batch_destroy(es_batch* b)
     free_grids(b);
     cudaFree(b->d_counter);
     cudaFree(b->d_error);
+    cudaFree(b->d_retrace);
+    cudaFree(b->d_retrace_count);
     if (b->h_error) cudaFreeHost(b->h_error);
+    if (b->h_retrace_count) cudaFreeHost(b->h_retrace_count);
+    for (int k = 0; k < es_batch::kBranches; k++) {
+        if (b->branch[k]) cudaStreamDestroy(b->branch[k]);
+        if (b->join[k]) cudaEventDestroy(b->join[k]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return ES_OK;
@@ -589,11 +1000,16 @@ es_status es_batch_set_tuning(es_batch* b, const es_batch_tuning* t)
         return bfail(b, ES_ERR_BAD_ARG, "blocks_per_sm must be 3 or 4 (got %d)", t->blocks_per_sm);
     if (t->precision != ES_PRECISION_FP64 && t->precision != ES_PRECISION_SPLIT)
         return bfail(b, ES_ERR_BAD_ARG, "unknown precision %d", t->precision);
-    const bool items_change = t->chunk_iters != b->tuning.chunk_iters;
+    if (t->mode != ES_BATCH_PASS_NODES && t->mode != ES_BATCH_GRID && t->mode != ES_BATCH_PERSISTENT)
+        return bfail(b, ES_ERR_BAD_ARG, "unknown batch mode %d", t->mode);
+    auto item_orbits = [](const es_batch_tuning& x) {
+        return x.mode == ES_BATCH_PERSISTENT ? 32LL * x.chunk_iters : 32LL * es::kBatchWarps;
+    };
+    const bool items_change = item_orbits(*t) != item_orbits(b->tuning);
     b->tuning = *t;
     b->graph_dirty = true;
     if (items_change && b->has_instances) {
-        // work-item boundaries depend on chunk_iters: re-lay the table
+        // work-item boundaries depend on the mode and chunk_iters: re-lay the table
         std::vector<es_batch_instance> copy = b->inst;
         return es_batch_set_instances(b, copy.data(), (int32_t)copy.size());
     }
@@ -755,7 +1171,9 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return orbits_of(a) > orbits_of(c); });
 
-    const int64_t item_orbits = 32LL * b->tuning.chunk_iters;
+    const int64_t item_orbits =
+        b->tuning.mode == ES_BATCH_PERSISTENT ? 32LL * b->tuning.chunk_iters : 32LL * es::kBatchWarps;
+    b->pass_items.assign((size_t)n, 0);
     long long* hdr = reinterpret_cast<long long*>(b->h_table);
     es::BatchInstanceD* hi = reinterpret_cast<es::BatchInstanceD*>(b->h_table + b->inst_offset);
     b->factor.assign((size_t)n, {});
@@ -816,7 +1234,8 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
         d.fx_scale = fixed_point_scale(x.positions_per_row, x.particles_per_quadrant, max_wtau);
         hi[pos] = d;
         hdr[1 + pos] = items;
-        items += (L.n_orbits + item_orbits - 1) / item_orbits;
+        b->pass_items[(size_t)pos] = (L.n_orbits + item_orbits - 1) / item_orbits;
+        items += b->pass_items[(size_t)pos];
         total += L.n_orbits;
         b->factor[(size_t)k] = fac;
         b->fx_scale[(size_t)k] = d.fx_scale;
@@ -829,6 +1248,12 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
     b->total_orbits = total;
     b->total_items = items;
     b->has_instances = true;
+    // pass records are kernel parameters in this mode: record the graph again
+    if (b->tuning.mode == ES_BATCH_PASS_NODES) b->graph_dirty = true;
+    // Re-traced orbits are a small fraction (observed ~0.05%); the list starts
+    // at 1/1024 of the run and grows on overflow (es_batch_collect re-runs).
+    if (b->tuning.precision == ES_PRECISION_SPLIT)
+        if ((st = ensure_retrace(b, total / 1024 + 262144)) != ES_OK) return st;
     return ES_OK;
 }
 
@@ -837,7 +1262,11 @@ es_status es_batch_enqueue(es_batch* b)
     es_status st = bind_batch(b);
     if (st != ES_OK) return st;
     if (!b->has_instances) return bfail(b, ES_ERR_BAD_ARG, "es_batch_set_instances has not been called");
-    if (b->graph_dirty || !b->exec)
+    if (b->tuning.precision == ES_PRECISION_SPLIT && b->retrace_cap == 0)
+        if ((st = ensure_retrace(b, b->total_orbits / 1024 + 262144)) != ES_OK) return st;
+    if (b->tuning.mode == ES_BATCH_GRID && b->total_items > 0x7fffffffLL)
+        return bfail(b, ES_ERR_BAD_ARG, "more than 2^31 - 1 work items: use another batch mode or split the batch");
+    if (b->graph_dirty || !b->exec || (b->tuning.mode == ES_BATCH_GRID && b->captured_items != b->total_items))
         if ((st = capture(b)) != ES_OK) return st;
     ES_BCUDA(cudaGraphLaunch(b->exec, b->stream), "batch graph launch");
     b->launches++;
@@ -850,6 +1279,16 @@ es_status es_batch_collect(es_batch* b, double* out_sigma, es_metrics* out_metri
     if (st != ES_OK) return st;
     if (!b->has_instances) return bfail(b, ES_ERR_BAD_ARG, "es_batch_set_instances has not been called");
     ES_BCUDA(cudaStreamSynchronize(b->stream), "batch synchronize");
+    if (*b->h_error & es::kErrRetraceOverflow) {
+        // the list was too short for this run: grow it to fit and run again
+        const long long need = (long long)*b->h_retrace_count;
+        if ((st = ensure_retrace(b, need + need / 4 + 1024)) != ES_OK) return st;
+        b->retrace_regrows++;
+        if ((st = es_batch_enqueue(b)) != ES_OK) return st;
+        ES_BCUDA(cudaStreamSynchronize(b->stream), "batch synchronize");
+        if (*b->h_error & es::kErrRetraceOverflow)
+            return bfail(b, ES_ERR_LAUNCH, "split precision: the FP64 re-trace list overflowed twice");
+    }
     const int h_err = *b->h_error;
     if (h_err & es::kErrWalkCap)
         return bfail(b, ES_ERR_WALK_CAP, "an orbit exceeded the cell-walk step bound (its lifetime was set to 0)");

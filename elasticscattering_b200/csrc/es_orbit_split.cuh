@@ -40,6 +40,62 @@ constexpr float kTwoPiF = 6.2831853071795864769f;
 constexpr float kPiF = 3.1415926535897932385f;
 constexpr float kGuard = 4e-6f;        // angle guard (rad): ~40x the FP32 angle error
 
+// Where the walk reads its per-pass constants. LaunchFields: from a
+// LifetimeLaunch passed as the kernel parameter, whose fields are constant-bank
+// operands and cost no registers. SharedFields: from a LifetimeLaunch in shared
+// memory (the batched kernels), loaded where the compiler chooses.
+struct LaunchFields {
+    const LifetimeLaunch& P;
+    __device__ __forceinline__ const int* cell_end() const { return P.cell_end; }
+    __device__ __forceinline__ const float2* imps32() const { return P.imps32; }
+    __device__ __forceinline__ const double2* imps() const { return P.imps; }
+    __device__ __forceinline__ const PhaseOrbit* phase() const { return P.phase; }
+    __device__ __forceinline__ int* error() const { return P.error; }
+    __device__ __forceinline__ double spawn_start() const { return P.spawn_start; }
+    __device__ __forceinline__ double spawn_size() const { return P.spawn_size; }
+    __device__ __forceinline__ double cell_size() const { return P.cell_size; }
+    __device__ __forceinline__ double imp_radius() const { return P.imp_radius; }
+    __device__ __forceinline__ double speed() const { return P.speed; }
+    __device__ __forceinline__ double radius() const { return P.radius; }
+    __device__ __forceinline__ double radius_sq() const { return P.radius_sq; }
+    __device__ __forceinline__ double w() const { return P.w; }
+    __device__ __forceinline__ double dist() const { return P.dist; }
+    __device__ __forceinline__ double off_x() const { return P.off_x; }
+    __device__ __forceinline__ double off_y() const { return P.off_y; }
+    __device__ __forceinline__ int cpr() const { return P.cpr; }
+    __device__ __forceinline__ int dim() const { return P.dim; }
+    __device__ __forceinline__ int n_phase() const { return P.n_phase; }
+    __device__ __forceinline__ int clockwise() const { return P.clockwise; }
+    __device__ __forceinline__ int coherent() const { return P.coherent; }
+    __device__ __forceinline__ int walk_cap() const { return P.walk_cap; }
+};
+
+struct SharedFields {
+    const LifetimeLaunch* P;  // shared memory
+    __device__ __forceinline__ const int* cell_end() const { return P->cell_end; }
+    __device__ __forceinline__ const float2* imps32() const { return P->imps32; }
+    __device__ __forceinline__ const double2* imps() const { return P->imps; }
+    __device__ __forceinline__ const PhaseOrbit* phase() const { return P->phase; }
+    __device__ __forceinline__ int* error() const { return P->error; }
+    __device__ __forceinline__ double spawn_start() const { return P->spawn_start; }
+    __device__ __forceinline__ double spawn_size() const { return P->spawn_size; }
+    __device__ __forceinline__ double cell_size() const { return P->cell_size; }
+    __device__ __forceinline__ double imp_radius() const { return P->imp_radius; }
+    __device__ __forceinline__ double speed() const { return P->speed; }
+    __device__ __forceinline__ double radius() const { return P->radius; }
+    __device__ __forceinline__ double radius_sq() const { return P->radius_sq; }
+    __device__ __forceinline__ double w() const { return P->w; }
+    __device__ __forceinline__ double dist() const { return P->dist; }
+    __device__ __forceinline__ double off_x() const { return P->off_x; }
+    __device__ __forceinline__ double off_y() const { return P->off_y; }
+    __device__ __forceinline__ int cpr() const { return P->cpr; }
+    __device__ __forceinline__ int dim() const { return P->dim; }
+    __device__ __forceinline__ int n_phase() const { return P->n_phase; }
+    __device__ __forceinline__ int clockwise() const { return P->clockwise; }
+    __device__ __forceinline__ int coherent() const { return P->coherent; }
+    __device__ __forceinline__ int walk_cap() const { return P->walk_cap; }
+};
+
 __device__ __forceinline__ float wrap2pi(float a) { return a - kTwoPiF * floorf(a * (1.0f / kTwoPiF)); }
 
 // Advance (angle travelled since the start, in [0, 2pi)) of position angle psi.
@@ -145,14 +201,14 @@ struct SplitCounters {
 };
 
 // The winning disk's reference time (FP64) and the bound clamp.
-__device__ __forceinline__ double finish_hit(const LifetimeLaunch& P, const OrbitD& o, int win_k, int alt_k,
-                                             int& flags)
+template <class F>
+__device__ __forceinline__ double finish_hit(const F& f, const OrbitD& o, int win_k, int alt_k, int& flags)
 {
-    const double2 q = __ldg(P.imps + win_k);
-    double t = first_cross_angle_open(o, dv2{q.x, q.y}, P.imp_radius) / P.w;
+    const double2 q = __ldg(f.imps() + win_k);
+    double t = first_cross_angle_open(o, dv2{q.x, q.y}, f.imp_radius()) / f.w();
     if (alt_k >= 0) {
-        const double2 a = __ldg(P.imps + alt_k);
-        const double t2 = first_cross_angle_open(o, dv2{a.x, a.y}, P.imp_radius) / P.w;
+        const double2 a = __ldg(f.imps() + alt_k);
+        const double t2 = first_cross_angle_open(o, dv2{a.x, a.y}, f.imp_radius()) / f.w();
         t = (t < t2) ? t : t2;
     }
     flags = kTraceOk;
@@ -165,13 +221,12 @@ __device__ __forceinline__ double finish_hit(const LifetimeLaunch& P, const Orbi
 
 // FP32 walk of one orbit. Returns kSplitDone with `out` set (and flags for the
 // metrics), or kSplitRetrace when the orbit must be re-traced in FP64.
-__device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD& o, dv2 pos, SplitCounters& cnt,
-                                           int& flags, double& out)
+template <class F>
+__device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos, SplitCounters& cnt, int& flags,
+                                           double& out)
 {
-    const double L = P.cell_size;
-    const int cpr = P.cpr;
     const double r64 = o.radius;
-    const double ir64 = P.imp_radius;
+    const double ir64 = f.imp_radius();
     const float r = (float)r64;
     const float inv_r = (float)(1.0 / r64);
     const float ir = (float)ir64;
@@ -186,26 +241,26 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
     const float dir = o.clockwise ? -1.0f : 1.0f;
     const float psi0 = (float)(o.clockwise ? o.particle_angle - kHALF_PI : o.particle_angle + kHALF_PI);
 
-    int cx = (int)((pos.x - P.spawn_start) / P.spawn_size * (double)cpr);
-    int cy = (int)((pos.y - P.spawn_start) / P.spawn_size * (double)cpr);
+    int cx = (int)((pos.x - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
+    int cy = (int)((pos.y - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
 
     // Start-cell InsideImpurity scan (lifetime.h:90-99), FP32 with an FP64 band.
     {
-        const int c = cy * cpr + cx;
-        const int k0 = (c == 0) ? 0 : __ldg(P.cell_end + c - 1);
-        const int k1 = __ldg(P.cell_end + c);
-        const float plx = (float)(pos.x - (P.spawn_start + cx * L));
-        const float ply = (float)(pos.y - (P.spawn_start + cy * L));
+        const int c = cy * f.cpr() + cx;
+        const int k0 = (c == 0) ? 0 : __ldg(f.cell_end() + c - 1);
+        const int k1 = __ldg(f.cell_end() + c);
+        const float plx = (float)(pos.x - (f.spawn_start() + cx * f.cell_size()));
+        const float ply = (float)(pos.y - (f.spawn_start() + cy * f.cell_size()));
         const float ir2 = ir * ir;
         for (int k = k0; k < k1; k++) {
-            const float2 q = __ldg(P.imps32 + k);
+            const float2 q = __ldg(f.imps32() + k);
             const float dx = plx - q.x, dy = ply - q.y;
             const float d2 = fmaf(dx, dx, dy * dy);
             cnt.start_tests += 1;
             bool inside = d2 < ir2;
             if (fabsf(d2 - ir2) <= 1e-4f * ir2) {
-                const double2 q64 = __ldg(P.imps + k);
-                inside = inside_impurity(pos, dv2{q64.x, q64.y}, ir64);
+                const double2 q64 = __ldg(f.imps() + k);
+                inside = inside_impurity(pos, dv2{q64.x, q64.y}, f.imp_radius());
             }
             if (inside) {
                 flags = kTraceInside;
@@ -219,13 +274,16 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
     // y-lo, y-hi), two per line, -1 when the line misses the circle. Moving to
     // a neighbour keeps three of the four lines, so one line is new per step.
     float la[4], lb[4];
-    const double llx0 = P.spawn_start + cx * L, lly0 = P.spawn_start + cy * L;
+    {
+        const double L = f.cell_size();
+        const double llx0 = f.spawn_start() + cx * L, lly0 = f.spawn_start() + cy * L;
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-        const double c64 = e == 0 ? llx0 - o.center.x
-                                  : (e == 1 ? (llx0 + L) - o.center.x
-                                            : (e == 2 ? lly0 - o.center.y : (lly0 + L) - o.center.y));
-        line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+        for (int e = 0; e < 4; e++) {
+            const double c64 = e == 0 ? llx0 - o.center.x
+                                      : (e == 1 ? (llx0 + L) - o.center.x
+                                                : (e == 2 ? lly0 - o.center.y : (lly0 + L) - o.center.y));
+            line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+        }
     }
 
     float a_cur = 0.0f;        // advance at which the current cell was entered
@@ -234,7 +292,6 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
     int steps = 0;
 
     for (;;) {
-        const double llx = P.spawn_start + cx * L, lly = P.spawn_start + cy * L;
 
         // ---- exit of this cell: first edge-line crossing after a_cur ----
         float ex = kTwoPiF, ex2 = kTwoPiF;
@@ -281,19 +338,21 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
         if (ex_line == 1) nx += 1;
         if (ex_line == 2) ny -= 1;
         if (ex_line == 3) ny += 1;
-        const bool final_visit = ex_line < 0 || nx < 0 || ny < 0 || nx >= cpr || ny >= cpr;
+        const bool final_visit = ex_line < 0 || nx < 0 || ny < 0 || nx >= f.cpr() || ny >= f.cpr();
 
         // ---- disks of this cell ----
-        const int c = cy * cpr + cx;
-        const int k0 = (c == 0) ? 0 : __ldg(P.cell_end + c - 1);
-        const int k1 = __ldg(P.cell_end + c);
+        const int c = cy * f.cpr() + cx;
+        const int k0 = (c == 0) ? 0 : __ldg(f.cell_end() + c - 1);
+        const int k1 = __ldg(f.cell_end() + c);
         cnt.cells += 1;
         cnt.imps += k1 - k0;
-        const float ox = (float)(llx - o.center.x), oy = (float)(lly - o.center.y);
+        const float ox = (float)((f.spawn_start() + cx * f.cell_size()) - o.center.x);
+        const float oy = (float)((f.spawn_start() + cy * f.cell_size()) - o.center.y);
+        const float2* const imps32 = f.imps32();
         float v1 = 3.0e38f, v2 = 3.0e38f, v3 = 3.0e38f;  // best three crossing advances of this visit
         int k1st = -1, k2nd = -1;
         for (int k = k0; k < k1; k++) {
-            const float2 q = __ldg(P.imps32 + k);
+            const float2 q = __ldg(imps32 + k);
             const float dx = q.x + ox, dy = q.y + oy;
             const float d2 = fmaf(dx, dx, dy * dy);
             if (d2 < lo2 - eps2 || d2 > hi2 + eps2) continue;
@@ -302,9 +361,9 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
             float a;
             if (fabsf(fabsf(delta) - ir) <= band_d) {
                 // grazing disk: CirclesCross and the crossing angle in FP64
-                const double2 q64 = __ldg(P.imps + k);
-                if (!circles_cross(o, dv2{q64.x, q64.y}, ir64)) continue;
-                a = (float)first_cross_angle_open(o, dv2{q64.x, q64.y}, ir64);
+                const double2 q64 = __ldg(f.imps() + k);
+                if (!circles_cross(o, dv2{q64.x, q64.y}, f.imp_radius())) continue;
+                a = (float)first_cross_angle_open(o, dv2{q64.x, q64.y}, f.imp_radius());
             } else {
                 if (!(fabsf(delta) < ir)) continue;
                 // crossing half-angle at the orbit centre:
@@ -336,7 +395,7 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
         global_a = fminf(global_a, v1);
 
         if (!final_visit && !(global_a < ex + kGuard)) {
-            if (++steps >= P.walk_cap) return kSplitRetrace;
+            if (++steps >= f.walk_cap()) return kSplitRetrace;
             // Enter the neighbour: the crossed line becomes its opposite line,
             // the parallel line moves by one cell, the other two are shared.
             entry_line = ex_line ^ 1;
@@ -345,7 +404,8 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
             cx = nx;
             cy = ny;
             {
-                const double nllx = P.spawn_start + cx * L, nlly = P.spawn_start + cy * L;
+                const double L = f.cell_size();
+                const double nllx = f.spawn_start() + cx * L, nlly = f.spawn_start() + cy * L;
                 const int e = ex_line;  // the new cell's line on the far side has the same index
                 const double c64 = e == 0 ? nllx - o.center.x
                                           : (e == 1 ? (nllx + L) - o.center.x
@@ -378,50 +438,56 @@ __device__ __forceinline__ int trace_split(const LifetimeLaunch& P, const OrbitD
         // crossings the geometry accepts: clockwise in the final visit,
         // counter-clockwise in the first. The FP64 walk reproduces that.
         if (o.particle_angle < 0.0 && (o.clockwise ? final_visit : entry_line < 0)) return kSplitRetrace;
-        out = finish_hit(P, o, k1st, v2 < v1 + kGuard ? k2nd : -1, flags);
+        out = finish_hit(f, o, k1st, v2 < v1 + kGuard ? k2nd : -1, flags);
         return kSplitDone;
     }
 }
 
 // Orbit g of pass P (CreateParticle, src/sim/es/lifetime.h:36-58, with the
 // host-tabulated phase constants).
-__device__ __forceinline__ OrbitD make_orbit(const LifetimeLaunch& P, long long g, dv2& pos)
+template <class F>
+__device__ __forceinline__ OrbitD make_orbit(const F& f, long long g, dv2& pos)
 {
-    const int v = (int)(g % P.n_phase);
-    const long long pidx = g / P.n_phase;
-    const int i = (int)(pidx % P.dim);
-    const int j = (int)(pidx / P.dim);
-    pos = dv2{(double)i * P.dist + P.off_x, (double)j * P.dist + P.off_y};
-    const PhaseOrbit ph = P.phase[v];
+    const int v = (int)(g % f.n_phase());
+    const long long pidx = g / f.n_phase();
+    const int i = (int)(pidx % f.dim());
+    const int j = (int)(pidx / f.dim());
+    pos = dv2{(double)i * f.dist() + f.off_x(), (double)j * f.dist() + f.off_y()};
+    const PhaseOrbit ph = f.phase()[v];
     OrbitD o;
-    o.radius = P.radius;
-    o.radius_sq = P.radius_sq;
-    o.clockwise = P.clockwise != 0;
-    const double shift_x = (ph.vel_y * P.radius) / P.speed;
-    const double shift_y = (-ph.vel_x * P.radius) / P.speed;
+    o.radius = f.radius();
+    o.radius_sq = f.radius_sq();
+    o.clockwise = f.clockwise() != 0;
+    const double shift_x = (ph.vel_y * o.radius) / f.speed();
+    const double shift_y = (-ph.vel_x * o.radius) / f.speed();
     o.center = o.clockwise ? dv2{pos.x - shift_x, pos.y - shift_y} : dv2{pos.x + shift_x, pos.y + shift_y};
-    o.bound_time = P.coherent ? kINF : ph.bound_dphi / P.w;
+    o.bound_time = f.coherent() ? kINF : ph.bound_dphi / f.w();
     o.particle_angle = ph.phi;
     return o;
 }
 
+__device__ __forceinline__ OrbitD make_orbit(const LifetimeLaunch& P, long long g, dv2& pos)
+{
+    return make_orbit(LaunchFields{P}, g, pos);
+}
+
 // The split walk of orbit g. Returns true when the orbit must be re-traced in
 // FP64 (cnt and flags are then cleared); otherwise lt holds its lifetime.
-__device__ __forceinline__ bool split_orbit(const LifetimeLaunch& P, long long g, SplitCounters& cnt, int& flags,
-                                            double& lt)
+template <class F>
+__device__ __forceinline__ bool split_orbit(const F& f, long long g, SplitCounters& cnt, int& flags, double& lt)
 {
     dv2 pos;
-    const OrbitD o = make_orbit(P, g, pos);
+    const OrbitD o = make_orbit(f, g, pos);
     cnt = SplitCounters{0, 0, 0, 0};
     flags = kTraceOk;
     lt = 0.0;
-    const int cx = (int)((pos.x - P.spawn_start) / P.spawn_size * (double)P.cpr);
-    const int cy = (int)((pos.y - P.spawn_start) / P.spawn_size * (double)P.cpr);
-    if (cx < 0 || cy < 0 || cx >= P.cpr || cy >= P.cpr) {
-        atomicOr(P.error, kErrStartCell);
+    const int cx = (int)((pos.x - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
+    const int cy = (int)((pos.y - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
+    if (cx < 0 || cy < 0 || cx >= f.cpr() || cy >= f.cpr()) {
+        atomicOr(f.error(), kErrStartCell);
         return false;
     }
-    if (trace_split(P, o, pos, cnt, flags, lt) == kSplitRetrace) {
+    if (trace_split(f, o, pos, cnt, flags, lt) == kSplitRetrace) {
         cnt = SplitCounters{0, 0, 0, 0};
         flags = kTraceOk;
         return true;

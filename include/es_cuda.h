@@ -265,11 +265,23 @@ typedef struct es_batch_instance {
     double temperatures[ES_BATCH_MAX_T];
 } es_batch_instance;
 
+/* How a batch maps its passes onto kernels. In every mode one graph replay
+ * runs the whole batch; the autotuner picks the mode. */
+typedef enum es_batch_mode {
+    ES_BATCH_PASS_NODES = 0,  /* one kernel node per pass on parallel graph branches, the pass record
+                                 as kernel parameter; one block per 256 orbits */
+    ES_BATCH_GRID = 1,        /* one kernel over all passes, one block per 256 orbits, each block looks
+                                 its pass up in the device table */
+    ES_BATCH_PERSISTENT = 2   /* one persistent kernel: warps take work items of 32 * chunk_iters
+                                 orbits of any pass from a global counter */
+} es_batch_mode;
+
 /* Launch choices of a batch (picked by the autotuner). */
 typedef struct es_batch_tuning {
-    int32_t chunk_iters;    /* orbits per work item = 32 * chunk_iters */
-    int32_t blocks_per_sm;  /* resident blocks of 256 threads per SM: 3 or 4 */
+    int32_t chunk_iters;    /* ES_BATCH_PERSISTENT: orbits per work item = 32 * chunk_iters */
+    int32_t blocks_per_sm;  /* resident blocks of 256 threads per SM: 3 or 4 (register budget) */
     int32_t precision;      /* es_precision */
+    int32_t mode;           /* es_batch_mode */
 } es_batch_tuning;
 
 es_status es_batch_create(int32_t device_ordinal, es_batch** out);
