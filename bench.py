@@ -104,6 +104,76 @@ def reference_cpu_sample(wname: str, rows_per_proc: int, procs: int) -> dict:
                       f"(oracle/_ref)"}
 
 
+def _ref_worker_pass(p: dict):
+    """One host process: the reference's CPU code on rows [j0, j1) of the given
+    (sample, field, sector) passes. Returns (orbits, seconds)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as O
+    lib = O.ref()
+    g = lib.ref_grid_new_seed(p["seed"], p["L"], p["ext"], p["density"], p["r"], p["tcp"])
+    orbits, secs = 0, 0.0
+    for coh in (1, 0):
+        sim = lib.ref_sim_new(g, p["dim"], p["ppq"], p["tau"], p["alpha"], int(p["cw"]), p["speed"], p["L"], p["ext"])
+        lib.ref_sim_init_sample(sim, coh)
+        for B in p["fields"]:
+            t0 = time.perf_counter()
+            orbits += lib.ref_sim_lifetimes_rows(sim, float(B), p["j0"], p["j1"], None, None)
+            secs += time.perf_counter() - t0
+        lib.ref_sim_free(sim)
+    lib.ref_grid_free(g)
+    return orbits, secs
+
+
+def reference_cpu_batched(wl, tcp_for, procs: int) -> dict:
+    """The reference CPU path on a bounded sample of a batched sweep: process k
+    takes one start-position row of sample k (mod the sample count) at the
+    sweep's smallest, middle and largest field, both sectors."""
+    fields = sorted(wl.fields)
+    pick = [fields[0], fields[len(fields) // 2], fields[-1]]
+    jobs = []
+    for k in range(procs):
+        s = wl.samples[k % len(wl.samples)]
+        j0 = (k * 7919) % s.dim
+        jobs.append({"seed": s.seed, "L": wl.region_size, "ext": wl.region_extends, "density": s.density,
+                     "r": wl.impurity_radius, "tcp": tcp_for(s.density), "dim": s.dim, "ppq": wl.phi_steps,
+                     "tau": wl.tau, "alpha": wl.alpha, "cw": wl.clockwise, "speed": wl.particle_speed,
+                     "fields": pick, "j0": j0, "j1": j0 + 1})
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker_pass, jobs)
+    orbits = sum(r[0] for r in res)
+    secs = max(r[1] for r in res)
+    return {"orbits": orbits, "seconds": secs, "rate": orbits / secs, "procs": procs,
+            "sample": f"{wl.name}: 1 start-position row of one sample per process x {procs} processes, "
+                      f"fields {pick} x 2 sectors, reference SimulationCPU code (oracle/_ref)"}
+
+
+def run_reference_batched(args) -> None:
+    """Reference arm of the batched sweep: its CPU code on bounded row samples."""
+    wl = workloads.config2(n_samples=max(64, args.samples), n_fields=args.fields)
+    wl.samples = wl.samples[:args.samples]
+    wl.name = f"config2-{args.samples}x{args.fields}x3"
+    procs = os.cpu_count() or 1
+    tcp = lambda d: wl.target_cell_population  # noqa: E731  (the reference's config value)
+    for _ in range(args.warmup):
+        reference_cpu_batched(wl, tcp, procs)
+    steps = [reference_cpu_batched(wl, tcp, procs) for _ in range(args.steps)]
+    orbits = sum(s["orbits"] for s in steps)
+    secs = sum(s["seconds"] for s in steps)
+    rate = orbits / secs
+    orbits_per_point = wl.orbits / max(1, wl.sigma_points)
+    print(json.dumps({
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+        "data": "synthetic (seeded impurity fields; per-sample start grid and density drawn with seed 12345)",
+        "config": {"workload": wl.name, "sample": steps[0]["sample"]},
+        "sigma_points_per_sec": rate / orbits_per_point,
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": procs, "kind": "reference", "sample": steps[0]["sample"]},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -111,6 +181,9 @@ def run_reference(args) -> None:
     ref_so = ROOT / "oracle" / "_ref" / "libes_ref.so"
     if not ref_so.exists():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libes_ref.so was not built here"}))
+        return
+    if args.workload == "config2":
+        run_reference_batched(args)
         return
     w = workloads.WORKLOADS[args.workload]()
     procs = os.cpu_count() or 1
@@ -455,9 +528,213 @@ def e2e_through_api(args, w, grid, sw, world, dist, N, torch) -> dict:
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
 
+def run_batched(args) -> None:
+    """The batched sweep (config 2): samples x fields x temperatures with per-sample
+    start grids and densities, one graph replay per step, autotuned cell sizes and
+    launch shape. Reports the split path, the FP64 batch of the same passes (the
+    per-result error), the plain per-pass FP64 path on a subset, and the
+    reference CPU code on a bounded sample."""
+    import torch
+    import torch.distributed as dist
+    from concurrent.futures import ThreadPoolExecutor
+
+    from elasticscattering_b200 import Grid, SimulationCUDA, autotune
+    from elasticscattering_b200 import _native as N
+    from elasticscattering_b200.batch import BatchSweep, incoherent_temperature, sweep_passes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = local
+    # every rank runs its own `samples` samples of the draw (weak scaling)
+    wl = workloads.config2(n_samples=max(64, args.samples * world), n_fields=args.fields)
+    wl.samples = wl.samples[rank * args.samples:(rank + 1) * args.samples]
+    wl.name = f"config2-{args.samples}x{args.fields}x3"
+
+    t_tune = time.perf_counter()
+    tune = autotune.tune_sweep(wl, device=dev, cache=args.tune_cache, force=args.retune)
+    tune_wall = time.perf_counter() - t_tune
+    tcp_for = tune.tcp_for
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and (ROOT / "oracle/_ref/libes_ref.so").exists():
+        cpu = reference_cpu_batched(wl, tcp_for, os.cpu_count() or 1)
+
+    def build(s):
+        return Grid.from_seed(s.seed, wl.region_size, wl.region_extends, s.density, wl.impurity_radius,
+                              tcp_for(s.density))
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:
+        grids = list(ex.map(build, wl.samples))
+    grid_build_s = time.perf_counter() - t0
+    cell = {s.index: g.info().cell_size for s, g in zip(wl.samples, grids)}
+    uuid = ""
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+
+    bs = BatchSweep(dev, precision=N.ES_PRECISION_SPLIT, **tune.shape)
+    ids = {s.index: bs.add_grid(g) for s, g in zip(wl.samples, grids)}
+    passes = sweep_passes(wl, ids, cell)
+    bs.set_passes(passes)
+    n_pass = len(passes)
+    stream = torch.cuda.ExternalStream(bs.stream_handle())
+    for _ in range(args.warmup):
+        bs.run(with_metrics=False)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = bs.launch_count()
+    ms = []
+    with ClockSampler(uuid) as clocks:
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            bs.enqueue()
+            e1.record(stream)
+            out_split, mets = bs.collect()
+            ms.append(e0.elapsed_time(e1))
+    graph_replays = bs.launch_count() - launches0
+    total_ms = float(sum(ms))
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    orbits = bs.total_orbits
+    points = len(wl.samples) * len(wl.fields) * len(wl.temperatures)
+    kernels_per_replay = (n_pass if tune.shape["mode"] == N.ES_BATCH_PASS_NODES else 1) + 1
+    alg_flops = sum(lifetime_flops(m, 0) for m in mets) + FLOP_MODEL["per_orbit"] * orbits
+    retraced = sum(m["retraced_fp64"] for m in mets)
+
+    # the FP64 batch of the same passes: per-result error of the split path
+    bs.set_tuning(precision=N.ES_PRECISION_FP64)
+    bs.run(with_metrics=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    bs.enqueue()
+    e1.record(stream)
+    out_fp64, mets64 = bs.collect()
+    fp64_batch_ms = e0.elapsed_time(e1)
+    bs.close()
+    nt = len(wl.temperatures)
+    a, b = out_split[:, :nt, :], out_fp64[:, :nt, :]
+    rel = np.abs(a - b) / np.abs(b)
+    # sigma(B) points: coherent + incoherent per (sample, field, temperature)
+    pa, pb = a[0::2] + a[1::2], b[0::2] + b[1::2]
+    prel = np.abs(pa - pb) / np.abs(pb)
+    metrics_equal = all(x[k] == y[k] for x, y in zip(mets, mets64)
+                        for k in ("cells_passed", "impurities_tested", "particles_inside_impurity",
+                                  "particles_escaped", "particles_at_bound"))
+
+    # the plain per-pass FP64 path (one blocking ComputeSigmas per pass) on a subset,
+    # and the split batch on the same subset
+    n_sub = max(1, min(args.plain_samples, len(wl.samples)))
+    sub = wl.samples[:n_sub]
+    temps = [incoherent_temperature(x) for x in wl.temperatures]
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter()
+    plain = {}
+    for s, g in zip(sub, grids[:n_sub]):
+        st = next(p.settings for p in passes if p.grid == ids[s.index])
+        for coh in (True, False):
+            with SimulationCUDA(s.dim, wl.phi_steps, g.info(), device=dev, precision=N.ES_PRECISION_FP64) as sim:
+                sim.InitSample(g, st, coh)
+                for B in wl.fields:
+                    plain[(s.index, float(B), coh)] = sim.ComputeSigmas(float(B), temps)
+    plain_s = time.perf_counter() - t_plain
+    plain_pps = n_sub * len(wl.fields) * nt / plain_s
+    bsub = BatchSweep(dev, precision=N.ES_PRECISION_SPLIT, **tune.shape)
+    sid = {s.index: bsub.add_grid(g) for s, g in zip(sub, grids[:n_sub])}
+    sub_passes = sweep_passes(wl, sid, cell, samples=sub)
+    bsub.set_passes(sub_passes)
+    bsub.run(with_metrics=False)
+    torch.cuda.synchronize()
+    t_sub = time.perf_counter()
+    out_sub, _ = bsub.run(with_metrics=False)
+    sub_s = time.perf_counter() - t_sub
+    bsub.close()
+    sub_pps = n_sub * len(wl.fields) * nt / sub_s
+    grid_to_sample = {v: k for k, v in sid.items()}
+    worst_vs_plain = 0.0
+    for k, p in enumerate(sub_passes):
+        ref = plain[(grid_to_sample[p.grid], float(p.magnetic_field), bool(p.coherent))]
+        for ti, sg in enumerate(ref):
+            for c, v in enumerate((sg.xx, sg.xy)):
+                worst_vs_plain = max(worst_vs_plain, abs(out_sub[k, ti, c] - v) / abs(v))
+
+    # end to end through the public API with host buffers: grids copied in, results out
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter()
+    be = BatchSweep(dev, precision=N.ES_PRECISION_SPLIT, **tune.shape)
+    eid = {s.index: be.add_grid(g) for s, g in zip(wl.samples, grids)}
+    be.set_passes(sweep_passes(wl, eid, cell))
+    be.run(with_metrics=True)
+    e2e_s = time.perf_counter() - t_e2e
+    be.close()
+    h2d = sum(g.GetTotalImpurityCount() * 16 + g.GetCellsPerRow() ** 2 * 4 for g in grids)
+    d2h = n_pass * (N.ES_BATCH_MAX_T * 2 * 8 + 10 * 8)
+
+    peak32 = C.c_double(0.0)
+    N.check(N.cuda_lib().es_probe_fp32_fma(dev, C.byref(peak32)))
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    step_ms = total_ms / args.steps
+    achieved = alg_flops / (step_ms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": world * args.steps * orbits / (total_ms * 1e-3), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (split)",
+        "data": "synthetic (seeded impurity fields; per-sample start grid and density drawn with seed 12345)",
+        "config": {"workload": wl.name, "samples": len(wl.samples), "fields": len(wl.fields),
+                   "temperatures_K": wl.temperatures, "passes": n_pass, "orbits_per_step": orbits,
+                   "dims": sorted({s.dim for s in wl.samples}), "phi_steps": wl.phi_steps,
+                   "density_range": [min(s.density for s in wl.samples), max(s.density for s in wl.samples)],
+                   "l2": "inputs larger than L2 (the grids of all samples stay resident)"},
+        "sigma_points_per_sec": world * args.steps * points / (total_ms * 1e-3),
+        "tuning": {"shape": tune.shape, "tcp_by_density_class": list(zip(tune.density_edges[:-1], tune.tcp)),
+                   "tuner_seconds": round(tune.seconds, 1), "tuner_wall_this_run_s": round(tune_wall, 1)},
+        "gpu_launches": graph_replays * kernels_per_replay,
+        "graph_replays": graph_replays,
+        "retraced_fp64": retraced,
+        "clocks": clocks.summary(),
+        "roofline": {"bound": "fp32 pipe", "achieved": achieved, "peak": peak32.value, "unit": "TFLOP/s",
+                     "frac": achieved / peak32.value if peak32.value else None,
+                     "peak_source": "measured FP32 FMA rate (es_probe_fp32_fma)",
+                     "traffic": profiled_traffic("batch_kernel_config2.md"),
+                     "note": "algorithmic FP64-op model of TraceOrbit over the whole graph replay"},
+        "split_vs_fp64": {"results": int(rel.size), "max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
+                          "above_1e-6": int((rel > 1e-6).sum()), "sigma_points_max_rel": float(prel.max()),
+                          "metrics_equal": metrics_equal, "fp64_batch_ms": fp64_batch_ms,
+                          "per_instance_max_rel": [float(x) for x in rel.reshape(n_pass, -1).max(axis=1)]},
+        "plain_fp64_path": {"samples": n_sub, "points": n_sub * len(wl.fields) * nt, "seconds": plain_s,
+                            "points_per_sec": plain_pps, "split_batch_same_work_points_per_sec": sub_pps,
+                            "speedup_same_work": sub_pps / plain_pps, "max_rel_vs_plain_fp64": worst_vs_plain},
+        "host_grid_build_s": grid_build_s,
+        "e2e": {"value": orbits / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "seconds": e2e_s, "note": "BatchSweep with host grids: copies, graph record, run, readback"},
+    }
+    if cpu:
+        line["cpu_baseline"] = {"value": cpu["rate"], "unit": UNIT, "cores": cpu["procs"], "kind": "reference",
+                                "sample": cpu["sample"]}
+    print(json.dumps(line))
+
+
 def profiled_traffic(name: str):
-    """DRAM bytes per lifetime launch from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / ("lifetime_split_config1.md" if name == "split" else "lifetime_fp64_config1.md")
+    """DRAM bytes per launch from a committed ncu summary ("split", "fp64" or a
+    file name under profiles/), if present."""
+    if name.endswith(".md"):
+        p = ROOT / "profiles" / name
+    else:
+        p = ROOT / "profiles" / ("lifetime_split_config1.md" if name == "split" else "lifetime_fp64_config1.md")
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
@@ -476,12 +753,19 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["split", "fp64"], default="split")
-    ap.add_argument("--workload", default="config1", choices=sorted(workloads.WORKLOADS))
+    ap.add_argument("--workload", default="config1", choices=sorted(workloads.WORKLOADS) + ["config2"])
     ap.add_argument("--ref-rows", type=int, default=2, help="start-position rows per CPU process")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--samples", type=int, default=8, help="config2: impurity samples per GPU (64 = the full draw)")
+    ap.add_argument("--fields", type=int, default=32, help="config2: fields uniformly spaced 1-40 T")
+    ap.add_argument("--plain-samples", type=int, default=1, help="config2: samples timed on the plain FP64 path")
+    ap.add_argument("--tune-cache", default=None, help="config2: autotuner cache file")
+    ap.add_argument("--retune", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "config2":
+        run_batched(args)
     else:
         run_ours(args)
 

@@ -207,3 +207,28 @@ def test_batch_rejects_bad_instances(sweep_inputs, cuda_device):
         assert np.isfinite(out).all()
     finally:
         b.close()
+
+
+def test_autotuner_picks_from_measured_candidates_and_caches(tmp_path, cuda_device):
+    """A small sweep: the tuner times every candidate on pilot passes, keeps a
+    candidate per density class and one launch shape, and the second call
+    answers from the cache without timing anything."""
+    from elasticscattering_b200 import autotune
+    wl = workloads.config2(n_samples=4, n_fields=4)
+    wl.region_extends = workloads.orbit_diameter(SPEED, 8.0)
+    wl.fields = [8.0, 16.0, 24.0, 40.0]
+    for s in wl.samples:
+        s.density = min(s.density, 3e15)
+    cache = tmp_path / "tune.json"
+    shapes = autotune.SHAPE_CANDIDATES[:2] + autotune.SHAPE_CANDIDATES[4:]
+    r = autotune.tune_sweep(wl, device=cuda_device, n_classes=2, cache=cache, tcp_candidates=(6, 16),
+                            shape_candidates=shapes)
+    assert all(t in (6, 16) for t in r.tcp) and len(r.tcp) == 2
+    assert r.shape in [dict(s) for s in shapes]
+    cells = [t for t in r.trials if t["stage"] == "cell"]
+    assert len(cells) == 2 * 2 and all(t["ms"] > 0 for t in r.trials)
+    best = min((t for t in r.trials if t["stage"] == "shape"), key=lambda t: t["ms"])
+    assert {k: best[k] for k in r.shape} == r.shape
+    again = autotune.tune_sweep(wl, device=cuda_device, n_classes=2, cache=cache, tcp_candidates=(6, 16),
+                                shape_candidates=shapes)
+    assert again == r
