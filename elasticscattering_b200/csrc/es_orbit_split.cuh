@@ -39,6 +39,7 @@ namespace {
 constexpr float kTwoPiF = 6.2831853071795864769f;
 constexpr float kPiF = 3.1415926535897932385f;
 constexpr float kGuard = 4e-6f;        // angle guard (rad): ~40x the FP32 angle error
+constexpr double kPolarGuard = 4e-6;   // |x_line - x_centre| / r below which a vertical edge is re-traced
 
 // Where the walk reads its per-pass constants. LaunchFields: from a
 // LifetimeLaunch passed as the kernel parameter, whose fields are constant-bank
@@ -172,7 +173,10 @@ __device__ __forceinline__ void line_crossings(double c64, double r64, float inv
 // FP64 GetFirstCrossTime without the valid-range filter, as an angle: the
 // earlier of the two crossings' GetCrossAngle (src/sim/es/details.h:153-206).
 // Divided by w this is the reference's time for the disk that holds the first
-// crossing of the orbit.
+// crossing of the orbit. NaN when either crossing point's GetAngle is NaN:
+// for a point at the very top or bottom of the orbit, rounding can make
+// |y - c_y| / r exceed 1 and asin return NaN; the reference then drops that
+// point (AngleInRange is false for NaN), which only the FP64 walk reproduces.
 __device__ __forceinline__ double first_cross_angle_open(const OrbitD& o, dv2 ip, double ir)
 {
     const double qx = o.center.x - ip.x;
@@ -189,6 +193,7 @@ __device__ __forceinline__ double first_cross_angle_open(const OrbitD& o, dv2 ip
 #pragma unroll 1
     for (int k = 0; k < 2; k++) {
         const double a = cross_angle(o.particle_angle, get_angle(k == 0 ? p1 : p2, o), o.clockwise);
+        if (a != a) return a;
         a_min = (a_min < a) ? a_min : a;
     }
     return a_min;
@@ -273,7 +278,15 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
     // Crossing advances of the current cell's four edge lines (x-lo, x-hi,
     // y-lo, y-hi), two per line, -1 when the line misses the circle. Moving to
     // a neighbour keeps three of the four lines, so one line is new per step.
+    //
+    // A vertical line that passes within kPolarGuard r of the centre's x meets
+    // the circle within ~kPolarGuard rad of its top or bottom, where the
+    // reference's GetAngle (asin(dy / r), |dy| ~ r) can round to NaN and
+    // GetNextCell then drops that crossing (cell_grid.h:80-89) -- the walk stops
+    // or takes another edge. Such lines are marked in `polar` (bit = line) and a
+    // cell that has one hands the orbit to the FP64 re-trace.
     float la[4], lb[4];
+    unsigned polar = 0u;
     {
         const double L = f.cell_size();
         const double llx0 = f.spawn_start() + cx * L, lly0 = f.spawn_start() + cy * L;
@@ -283,6 +296,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
                                       : (e == 1 ? (llx0 + L) - o.center.x
                                                 : (e == 2 ? lly0 - o.center.y : (lly0 + L) - o.center.y));
             line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+            if (e < 2 && fabs(c64) < kPolarGuard * r64) polar |= 1u << e;
         }
     }
 
@@ -301,6 +315,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
         for (int e = 0; e < 4; e++) {
             float a1 = la[e], a2 = lb[e];
             if (a1 < 0.0f) continue;
+            if ((polar >> e) & 1u) ambiguous = true;  // crossing at the top or bottom of the orbit
             if (e == entry_line) {
                 // one of the two is the entry crossing itself
                 const float d1 = fabsf(a1 - a_cur), d2 = fabsf(a2 - a_cur);
@@ -330,6 +345,24 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
         if (ex_line >= 0) {
             if (ex - a_cur < kGuard) return kSplitRetrace;                                        // tiny arc
             if (ex2_line >= 0 && ex2_line != ex_line && ex2 - ex < kGuard) return kSplitRetrace;  // corner
+            // GetNextCell's corner rule (cell_grid.h:154-167) moves diagonally when
+            // the exit point lies within 1e-7 L of a perpendicular edge. Where the
+            // orbit runs almost parallel to that edge, the point can be that close
+            // while the edge's own crossing is far away in angle, so the exit
+            // line's two crossing points are located in FP64 and checked against
+            // both perpendicular edges (2x margin).
+            const double L = f.cell_size();
+            const double llx = f.spawn_start() + cx * L, lly = f.spawn_start() + cy * L;
+            const bool horiz = ex_line >= 2;
+            const double lv = horiz ? (ex_line == 2 ? lly : lly + L) : (ex_line == 0 ? llx : llx + L);
+            const double d = lv - (horiz ? o.center.y : o.center.x);
+            const double h = sqrt(fmax(o.radius_sq - d * d, 0.0));
+            const double c_perp = horiz ? o.center.x : o.center.y;
+            const double lo = horiz ? llx : lly;
+            const double tol = 2e-7 * L;
+            const double p1 = c_perp + h, p2 = c_perp - h;
+            if (fabs(p1 - lo) < tol || fabs(p1 - (lo + L)) < tol || fabs(p2 - lo) < tol || fabs(p2 - (lo + L)) < tol)
+                return kSplitRetrace;
         }
         // Next cell across the exit line; a final visit when the orbit comes
         // full circle or the next cell leaves the grid.
@@ -363,7 +396,9 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
                 // grazing disk: CirclesCross and the crossing angle in FP64
                 const double2 q64 = __ldg(f.imps() + k);
                 if (!circles_cross(o, dv2{q64.x, q64.y}, f.imp_radius())) continue;
-                a = (float)first_cross_angle_open(o, dv2{q64.x, q64.y}, f.imp_radius());
+                const double a64 = first_cross_angle_open(o, dv2{q64.x, q64.y}, f.imp_radius());
+                if (a64 != a64) return kSplitRetrace;  // a crossing point the reference drops
+                a = (float)a64;
             } else {
                 if (!(fabsf(delta) < ir)) continue;
                 // crossing half-angle at the orbit centre:
@@ -401,6 +436,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
             entry_line = ex_line ^ 1;
             la[entry_line] = la[ex_line];
             lb[entry_line] = lb[ex_line];
+            polar = (polar & ~(1u << entry_line)) | (((polar >> ex_line) & 1u) << entry_line);
             cx = nx;
             cy = ny;
             {
@@ -411,6 +447,8 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
                                           : (e == 1 ? (nllx + L) - o.center.x
                                                     : (e == 2 ? nlly - o.center.y : (nlly + L) - o.center.y));
                 line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+                polar &= ~(1u << e);
+                if (e < 2 && fabs(c64) < kPolarGuard * r64) polar |= 1u << e;
             }
             a_cur = ex;
             continue;
@@ -439,6 +477,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
         // counter-clockwise in the first. The FP64 walk reproduces that.
         if (o.particle_angle < 0.0 && (o.clockwise ? final_visit : entry_line < 0)) return kSplitRetrace;
         out = finish_hit(f, o, k1st, v2 < v1 + kGuard ? k2nd : -1, flags);
+        if (out != out) return kSplitRetrace;  // the winner's crossing point is one the reference drops
         return kSplitDone;
     }
 }

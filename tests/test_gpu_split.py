@@ -93,3 +93,46 @@ def test_split_config1_full_size(cuda_device):
     finally:
         plain.close()
         split.close()
+
+
+# (sample, sector, field index) of config-2 passes where the reference's own
+# rounding decides orbits: found by scanning split against plain FP64.
+REFERENCE_ROUNDING_CASES = [
+    # a vertical cell edge within ~1e-14 m of the orbit centre's x: the reference's
+    # GetAngle takes asin of a ratio that rounds past -1, gets NaN and drops that
+    # edge crossing, so the walk stops (an escape, lifetime 0)
+    (2, False, 3), (2, False, 6),
+    # an exit point within 1e-7 L of a perpendicular edge while the orbit runs almost
+    # parallel to it: GetNextCell's corner rule moves diagonally and the walk
+    # doubles back on itself
+    (0, True, 24), (2, False, 25), (2, True, 22),
+]
+
+
+@pytest.mark.parametrize("sample,coherent,field_index", REFERENCE_ROUNDING_CASES)
+def test_split_reproduces_reference_rounding_cases(cuda_device, sample, coherent, field_index):
+    """Config-2 passes (513^2 starts, 7-9e15 m^-2, cells of target population 8)
+    that contain orbits decided by the reference's rounding: the split path must
+    hand them to the FP64 re-trace, so every lifetime equals the plain path's,
+    bit for bit, and so do the walk metrics."""
+    wl = workloads.config2(n_samples=64)
+    s = wl.samples[sample]
+    B = wl.fields[field_index]
+    g = Grid.from_seed(s.seed, wl.region_size, wl.region_extends, s.density, wl.impurity_radius, 8)
+    st = make_settings(wl.tau, wl.alpha, wl.clockwise, wl.particle_speed, wl.region_size, wl.region_extends,
+                       s.density, wl.impurity_radius, 8)
+    plain = SimulationCUDA(s.dim, wl.phi_steps, g.info(), device=cuda_device, precision=N.ES_PRECISION_FP64)
+    split = SimulationCUDA(s.dim, wl.phi_steps, g.info(), device=cuda_device, precision=N.ES_PRECISION_SPLIT)
+    try:
+        plain.InitSample(g, st, coherent)
+        split.InitSample(g, st, coherent)
+        a, ma = plain.ComputeLifetimes(B)
+        b, mb = split.ComputeLifetimes(B)
+        r = compare(a, b)
+        assert r["bit_identical"] == 1.0, (B, r, mb["retraced_fp64"])
+        for k in ("cells_passed", "impurities_tested", "particles_inside_impurity", "particles_escaped",
+                  "particles_at_bound"):
+            assert ma[k] == mb[k], (B, k, ma[k], mb[k])
+    finally:
+        plain.close()
+        split.close()
