@@ -123,6 +123,18 @@ CUDA_API = {
     "es_batch_stream": (_vp, [_vp]),
     "es_batch_launch_count": (_i64, [_vp]),
     "es_batch_total_orbits": (_i64, [_vp]),
+    "es_mlp_param_count": (_i64, []),
+    "es_mlp_create": (_i32, [_i32, _i32, C.POINTER(_vp)]),
+    "es_mlp_destroy": (_i32, [_vp]),
+    "es_mlp_last_error": (C.c_char_p, [_vp]),
+    "es_mlp_set_params": (_i32, [_vp, _vp]),
+    "es_mlp_get_params": (_i32, [_vp, _vp]),
+    "es_mlp_set_dataset": (_i32, [_vp, _vp, _vp, _i64]),
+    "es_mlp_train": (_i32, [_vp, _i32, _i32, C.c_float, _u64, _vp]),
+    "es_mlp_gradients": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp]),
+    "es_mlp_predict": (_i32, [_vp, _vp, _i64, _vp, _vp, _vp]),
+    "es_mlp_launch_count": (_i64, [_vp]),
+    "es_mlp_stream": (_vp, [_vp]),
     "es_debug_trace": (_i32, [_vp, _d, _d, _i32, _i32, _d, _d, _d, _d, _d, _i32, _i32, C.POINTER(_d)]),
     "es_debug_next_cell": (_i32, [_vp, _d, _d, _d, _i32, _d, C.POINTER(ImpuritySettings), _vp, _vp,
                                   C.POINTER(_i32)]),
@@ -181,6 +193,12 @@ def check(status: int, ctx=None) -> None:
 def check_batch(status: int, batch) -> None:
     if status != ES_OK:
         msg = cuda_lib().es_batch_last_error(batch)
+        raise EsError(status, msg.decode() if msg else "")
+
+
+def check_mlp(status: int, mlp) -> None:
+    if status != ES_OK:
+        msg = cuda_lib().es_mlp_last_error(mlp)
         raise EsError(status, msg.decode() if msg else "")
 
 

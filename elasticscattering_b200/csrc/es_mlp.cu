@@ -1,0 +1,851 @@
+// es_mlp.cu - the learned surrogate: an ensemble of small MLPs that maps
+// (log B, T, log density, impurity radius, log tau) to (sigma_xx, sigma_xy) / sigma_0.
+//
+// No reference counterpart. Architecture 5 -> 256 x 4 -> 2, GELU, one network per
+// ensemble member. The four hidden layers (99.7% of the weights) run on the tensor
+// cores (mma.sync m16n8k16) with BF16 weights and activations and FP32
+// accumulation; the 256 -> 2 output head runs in FP32 on the FP32 master
+// weights and FP32 activations, because its 256 terms cancel into a small
+// output and BF16 rounding there measurably limited the fit (about 1% error in
+// sigma). FP32 master weights and Adam state. Training and inference are this
+// file's kernels only:
+//   - gemm_kernel<TA, TB, EPI>: C[m][n] = sum_k A(m, k) B(n, k) for one ensemble
+//     member per blockIdx.z, with A and B read either row- or column-wise so the
+//     forward pass (X W^T), the input gradient (dZ W) and the weight gradient
+//     (dZ^T X) are all the same kernel; the epilogue adds the bias and applies
+//     GELU (forward), multiplies by GELU'(Z) (input gradient) or stores FP32
+//     (weight gradient, output layer);
+//   - small elementwise kernels: minibatch gather, loss gradient, bias
+//     gradient, Adam, ensemble mean and spread.
+// Every minibatch and reduction order is fixed: training is bit-reproducible.
+#include "es_cuda.h"
+#include "es_internal.h"
+
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace es {
+namespace {
+
+constexpr int kIn = 5, kHidden = 256, kOut = 2, kLayers = 5;  // 4 hidden layers + output
+constexpr int kDims[kLayers + 1] = {kIn, kHidden, kHidden, kHidden, kHidden, kOut};
+
+constexpr int kBM = 64, kBN = 64, kBK = 32, kPad = 8;  // GEMM tile; 4 warps of 32 x 32
+
+enum Epilogue : int {
+    kEpiHidden = 0,  // Z = acc + b (FP32 out), A = GELU(Z) (BF16 out2)
+    kEpiLinear = 1,  // acc + b (FP32 out)
+    kEpiDGelu = 2,   // acc * GELU'(Zprev) (BF16 out2)
+    kEpiPlain = 3    // acc (FP32 out)
+};
+
+struct GemmArgs {
+    const __nv_bfloat16* A;
+    const __nv_bfloat16* B;
+    long long strideA, strideB;  // per ensemble member (elements); 0 = shared
+    int lda, ldb;
+    int M, N, K;
+    const float* bias;  // kEpiHidden / kEpiLinear
+    long long strideBias;
+    float* out;  // FP32 [M][N], row stride N
+    __nv_bfloat16* out2;  // BF16 [M][N], row stride N
+    long long strideOut;
+    const float* zprev;  // kEpiDGelu: pre-activations, [M][N]
+};
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+
+__device__ __forceinline__ float gelu_grad(float x)
+{
+    const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
+    return cdf + x * pdf;
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// C[m][n] = sum_k A(m, k) B(n, k); A(m, k) = TA ? A[k * lda + m] : A[m * lda + k],
+// B(n, k) = TB ? B[k * ldb + n] : B[n * ldb + k]. Out-of-range elements read as 0.
+template <bool TA, bool TB, int EPI>
+__global__ void __launch_bounds__(128) gemm_kernel(GemmArgs g)
+{
+    __shared__ __align__(16) __nv_bfloat16 As[kBM][kBK + kPad];
+    __shared__ __align__(16) __nv_bfloat16 Bs[kBN][kBK + kPad];
+    const int net = blockIdx.z;
+    const __nv_bfloat16* A = g.A + net * g.strideA;
+    const __nv_bfloat16* B = g.B + net * g.strideB;
+    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int grp = lane >> 2, tig = lane & 3;
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[i][j][c] = 0.0f;
+
+    for (int k0 = 0; k0 < g.K; k0 += kBK) {
+        // stage the tiles (64 x 32 each, 16 elements per thread)
+        for (int e = tid; e < kBM * kBK; e += 128) {
+            int r, c;
+            if (TA) { c = e / kBM; r = e % kBM; } else { r = e / kBK; c = e % kBK; }
+            const int m = m0 + r, k = k0 + c;
+            As[r][c] = (m < g.M && k < g.K) ? (TA ? A[(long long)k * g.lda + m] : A[(long long)m * g.lda + k]) : zero;
+        }
+        for (int e = tid; e < kBN * kBK; e += 128) {
+            int r, c;
+            if (TB) { c = e / kBN; r = e % kBN; } else { r = e / kBK; c = e % kBK; }
+            const int n = n0 + r, k = k0 + c;
+            Bs[r][c] = (n < g.N && k < g.K) ? (TB ? B[(long long)k * g.ldb + n] : B[(long long)n * g.ldb + k]) : zero;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kBK; kk += 16) {
+            unsigned af[2][4], bf[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int r = wm + i * 16 + grp;
+                af[i][0] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * tig]);
+                af[i][1] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * tig]);
+                af[i][2] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * tig + 8]);
+                af[i][3] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * tig + 8]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int n = wn + j * 8 + grp;
+                bf[j][0] = *reinterpret_cast<const unsigned*>(&Bs[n][kk + 2 * tig]);
+                bf[j][1] = *reinterpret_cast<const unsigned*>(&Bs[n][kk + 2 * tig + 8]);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], af[i], bf[j]);
+        }
+        __syncthreads();
+    }
+
+    // epilogue: element (row, col) of the 16 x 8 tile (i, j): c0, c1 at (grp, 2 tig + {0, 1}),
+    // c2, c3 at (grp + 8, 2 tig + {0, 1})
+    float* out = g.out ? g.out + net * g.strideOut : nullptr;
+    __nv_bfloat16* out2 = g.out2 ? g.out2 + net * g.strideOut : nullptr;
+    const float* bias = g.bias ? g.bias + net * g.strideBias : nullptr;
+    const float* zprev = g.zprev ? g.zprev + net * g.strideOut : nullptr;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int m = m0 + wm + i * 16 + grp + (c >= 2 ? 8 : 0);
+                const int n = n0 + wn + j * 8 + 2 * tig + (c & 1);
+                if (m >= g.M || n >= g.N) continue;
+                const long long o = (long long)m * g.N + n;
+                const float v = acc[i][j][c];
+                if (EPI == kEpiHidden) {
+                    const float z = v + bias[n];
+                    out[o] = z;
+                    out2[o] = __float2bfloat16(gelu(z));
+                } else if (EPI == kEpiLinear) {
+                    out[o] = v + bias[n];
+                } else if (EPI == kEpiDGelu) {
+                    out2[o] = __float2bfloat16(v * gelu_grad(zprev[o]));
+                } else {
+                    out[o] = v;
+                }
+            }
+}
+
+template <bool TA, bool TB, int EPI>
+cudaError_t gemm(const GemmArgs& g, int nets, cudaStream_t s)
+{
+    const dim3 grid((g.N + kBN - 1) / kBN, (g.M + kBM - 1) / kBM, nets);
+    gemm_kernel<TA, TB, EPI><<<grid, 128, 0, s>>>(g);
+    return cudaGetLastError();
+}
+
+// splitmix64: the minibatch index stream (counter-based, reproducible).
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Minibatch of member `net` at `step`: M rows drawn with replacement from the
+// member's bootstrap view of the dataset.
+__global__ void gather_kernel(const float* x, const float* y, long long n, int M, int cap, unsigned long long seed,
+                              long long step, __nv_bfloat16* xb, float* yb)
+{
+    const int net = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const unsigned long long key = mix64(seed ^ mix64((unsigned long long)step * 0x100000001B3ull + net * 0x9E37ull + i));
+    const long long row = (long long)(key % (unsigned long long)n);
+#pragma unroll
+    for (int k = 0; k < kIn; k++) xb[((long long)net * cap + i) * kIn + k] = __float2bfloat16(x[row * kIn + k]);
+#pragma unroll
+    for (int k = 0; k < kOut; k++) yb[((long long)net * cap + i) * kOut + k] = y[row * kOut + k];
+}
+
+// The output head (256 -> 2) in FP32: out = W4 GELU(Z3) + b4 with the FP32
+// master weights and FP32 activations. One warp per row, lanes over the 256
+// inputs, fixed shuffle tree.
+__global__ void head_forward_kernel(const float* z3, const float* w, const float* b, long long stride_p, int M,
+                                    int cap, float* out)
+{
+    const int net = blockIdx.y;
+    const int m = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (m >= M) return;
+    const float* z = z3 + ((long long)net * cap + m) * kHidden;
+    const float* W = w + net * stride_p;
+    float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kHidden / 32; i++) {
+        const int k = lane + 32 * i;
+        const float a = gelu(z[k]);
+        s0 += W[k] * a;
+        s1 += W[kHidden + k] * a;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+    }
+    if (lane == 0) {
+        const float* B = b + net * stride_p;
+        out[((long long)net * cap + m) * kOut + 0] = s0 + B[0];
+        out[((long long)net * cap + m) * kOut + 1] = s1 + B[1];
+    }
+}
+
+// Head backward, part 1: dZ3 = (dY W4) * GELU'(Z3), rounded to BF16 for the trunk's GEMMs.
+__global__ void head_backward_dz_kernel(const float* dy, const float* z3, const float* w, long long stride_p, int M,
+                                        int cap, __nv_bfloat16* dz3)
+{
+    const int net = blockIdx.y;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)M * kHidden) return;
+    const int m = (int)(e / kHidden), k = (int)(e % kHidden);
+    const float* W = w + net * stride_p;
+    const long long row = (long long)net * cap + m;
+    const float g = dy[row * kOut] * W[k] + dy[row * kOut + 1] * W[kHidden + k];
+    dz3[row * kHidden + k] = __float2bfloat16(g * gelu_grad(z3[row * kHidden + k]));
+}
+
+// Head backward, part 2: dW4[j][k] = sum_m dY[m][j] GELU(Z3[m][k]) and
+// db4[j] = sum_m dY[m][j], one thread per k (and per j for the bias), rows in order.
+__global__ void head_backward_w_kernel(const float* dy, const float* z3, int M, int cap, float* gw, float* gb,
+                                       long long stride_p)
+{
+    const int net = blockIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= kHidden) return;
+    float s0 = 0.0f, s1 = 0.0f;
+    for (int m = 0; m < M; m++) {
+        const long long row = (long long)net * cap + m;
+        const float a = gelu(z3[row * kHidden + k]);
+        s0 += dy[row * kOut] * a;
+        s1 += dy[row * kOut + 1] * a;
+    }
+    gw[net * stride_p + k] = s0;
+    gw[net * stride_p + kHidden + k] = s1;
+    if (k < kOut) {
+        float s = 0.0f;
+        for (int m = 0; m < M; m++) s += dy[((long long)net * cap + m) * kOut + k];
+        gb[net * stride_p + k] = s;
+    }
+}
+
+// Loss (mean squared error over M x kOut) and its FP32 gradient. One block per
+// member; fixed-order tree for the loss.
+__global__ void loss_kernel(const float* pred, const float* target, int M, int cap, float* dpred, float* loss)
+{
+    __shared__ float s[256];
+    const int net = blockIdx.x;
+    const float scale = 2.0f / (float)(M * kOut);
+    float acc = 0.0f;
+    for (int e = threadIdx.x; e < M * kOut; e += blockDim.x) {
+        const long long o = (long long)net * cap * kOut + e;
+        const float d = pred[o] - target[o];
+        acc += d * d;
+        dpred[o] = scale * d;
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) loss[net] = s[0] / (float)(M * kOut);
+}
+
+// db[n] = sum_m dZ[m][n] (BF16 values, FP32 sum in row order).
+__global__ void bias_grad_kernel(const __nv_bfloat16* dz, int M, int cap, int N, float* db, long long stride_db)
+{
+    const int net = blockIdx.y;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const __nv_bfloat16* d = dz + (long long)net * cap * N;
+    float s = 0.0f;
+    for (int m = 0; m < M; m++) s += __bfloat162float(d[(long long)m * N + n]);
+    db[net * stride_db + n] = s;
+}
+
+// Adam on the FP32 master parameters; refreshes the BF16 weight copies.
+__global__ void adam_kernel(float* p, const float* g, float* m1, float* m2, __nv_bfloat16* w16, const int* is_weight,
+                            long long n, float lr, float b1, float b2, float eps, float c1, float c2)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.0f - b1) * gi;
+    const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = b;
+    const float v = p[i] - lr * (a / c1) / (sqrtf(b / c2) + eps);
+    p[i] = v;
+    if (is_weight[i] >= 0) w16[is_weight[i]] = __float2bfloat16(v);
+}
+
+// Ensemble mean and spread (population standard deviation / |mean|) per query and output.
+__global__ void ensemble_kernel(const float* pred, int nets, long long Q, float* mean, float* spread)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Q * kOut) return;
+    float s = 0.0f;
+    for (int k = 0; k < nets; k++) s += pred[(long long)k * Q * kOut + e];
+    const float mu = s / (float)nets;
+    float v = 0.0f;
+    for (int k = 0; k < nets; k++) {
+        const float d = pred[(long long)k * Q * kOut + e] - mu;
+        v += d * d;
+    }
+    mean[e] = mu;
+    spread[e] = sqrtf(v / (float)nets) / fmaxf(fabsf(mu), 1e-30f);
+}
+
+__global__ void to_bf16_kernel(const float* x, __nv_bfloat16* y, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = __float2bfloat16(x[i]);
+}
+
+}  // namespace
+}  // namespace es
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+namespace {
+
+// Parameter layout of one member: for each layer l, W_l [N_l][K_l] then b_l [N_l].
+struct Layout {
+    long long w_off[es::kLayers], b_off[es::kLayers], w16_off[es::kLayers];
+    long long n_params = 0, n_weights = 0;
+    Layout()
+    {
+        for (int l = 0; l < es::kLayers; l++) {
+            const long long K = es::kDims[l], N = es::kDims[l + 1];
+            w_off[l] = n_params;
+            w16_off[l] = n_weights;
+            n_params += N * K;
+            n_weights += N * K;
+            b_off[l] = n_params;
+            n_params += N;
+        }
+    }
+};
+
+const Layout& layout()
+{
+    static const Layout L;
+    return L;
+}
+
+}  // namespace
+
+struct es_mlp {
+    int device = 0;
+    int nets = 0;
+    cudaStream_t stream = nullptr;
+    char err[512] = "";
+    int64_t launches = 0;
+    long long step = 0;
+    // parameters (FP32 master, Adam moments, gradients), BF16 weight copies
+    float* d_p = nullptr;
+    float* d_g = nullptr;
+    float* d_m1 = nullptr;
+    float* d_m2 = nullptr;
+    __nv_bfloat16* d_w16 = nullptr;
+    int* d_is_weight = nullptr;  // per parameter: index into w16 (per member) or -1
+    // dataset
+    float* d_x = nullptr;
+    float* d_y = nullptr;
+    long long n_data = 0;
+    // work buffers for `cap` rows per member
+    int cap = 0;
+    __nv_bfloat16* d_act[es::kLayers] = {};  // A_l: [nets][cap][K_l]
+    float* d_z[es::kLayers] = {};            // Z_l (hidden) / output (last): [nets][cap][N_l]
+    __nv_bfloat16* d_dz[es::kLayers] = {};   // dZ_l: [nets][cap][N_l]
+    float* d_yb = nullptr;                   // targets [nets][cap][kOut]
+    float* d_dy = nullptr;                   // output gradient [nets][cap][kOut], FP32
+    float* d_xin = nullptr;                  // query staging [cap][kIn], FP32
+    float* d_loss = nullptr;                 // [nets]
+    float* h_loss = nullptr;                 // pinned
+    float* d_mean = nullptr;
+    float* d_spread = nullptr;
+};
+
+namespace {
+
+es_status mfail(es_mlp* m, es_status st, const char* fmt, const char* what = "")
+{
+    snprintf(m->err, sizeof m->err, fmt, what);
+    return st;
+}
+
+#define ES_MCUDA(call, what)                                                                              \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess) {                                                                          \
+            snprintf(m->err, sizeof m->err, "%s: %s", what, cudaGetErrorString(e_));                      \
+            return e_ == cudaErrorMemoryAllocation ? ES_ERR_OOM : ES_ERR_LAUNCH;                          \
+        }                                                                                                 \
+    } while (0)
+
+void free_work(es_mlp* m)
+{
+    for (int l = 0; l < es::kLayers; l++) {
+        cudaFree(m->d_act[l]);
+        cudaFree(m->d_z[l]);
+        cudaFree(m->d_dz[l]);
+        m->d_act[l] = nullptr;
+        m->d_z[l] = nullptr;
+        m->d_dz[l] = nullptr;
+    }
+    cudaFree(m->d_yb);
+    cudaFree(m->d_dy);
+    cudaFree(m->d_xin);
+    cudaFree(m->d_mean);
+    cudaFree(m->d_spread);
+    m->d_yb = m->d_dy = m->d_xin = m->d_mean = m->d_spread = nullptr;
+    m->cap = 0;
+}
+
+es_status ensure_rows(es_mlp* m, long long rows)
+{
+    if (rows <= m->cap) return ES_OK;
+    if (rows > 4000000) return mfail(m, ES_ERR_BAD_ARG, "at most 4,000,000 rows per call");
+    free_work(m);
+    const long long E = m->nets;
+    for (int l = 0; l < es::kLayers; l++) {
+        const long long K = es::kDims[l], N = es::kDims[l + 1];
+        ES_MCUDA(cudaMalloc(&m->d_act[l], sizeof(__nv_bfloat16) * E * rows * K), "activations");
+        ES_MCUDA(cudaMalloc(&m->d_z[l], sizeof(float) * E * rows * N), "pre-activations");
+        ES_MCUDA(cudaMalloc(&m->d_dz[l], sizeof(__nv_bfloat16) * E * rows * N), "gradients");
+    }
+    ES_MCUDA(cudaMalloc(&m->d_yb, sizeof(float) * E * rows * es::kOut), "targets");
+    ES_MCUDA(cudaMalloc(&m->d_dy, sizeof(float) * E * rows * es::kOut), "output gradient");
+    ES_MCUDA(cudaMalloc(&m->d_xin, sizeof(float) * rows * es::kIn), "query staging");
+    ES_MCUDA(cudaMalloc(&m->d_mean, sizeof(float) * rows * es::kOut), "ensemble mean");
+    ES_MCUDA(cudaMalloc(&m->d_spread, sizeof(float) * rows * es::kOut), "ensemble spread");
+    m->cap = (int)rows;
+    return ES_OK;
+}
+
+es::GemmArgs args0() { return es::GemmArgs{}; }
+
+// Forward pass of every member on rows already staged in d_act[0] (BF16
+// [nets][rows][kIn], or [rows][kIn] shared when shared_input).
+cudaError_t forward(es_mlp* m, int rows, bool shared_input)
+{
+    const Layout& L = layout();
+    const long long P = L.n_params, W = L.n_weights;
+    cudaError_t e = cudaSuccess;
+    // the BF16 trunk on the tensor cores
+    for (int l = 0; l + 1 < es::kLayers && e == cudaSuccess; l++) {
+        const int K = es::kDims[l], N = es::kDims[l + 1];
+        es::GemmArgs g = args0();
+        g.A = m->d_act[l];
+        g.strideA = (l == 0 && shared_input) ? 0 : (long long)m->cap * K;
+        g.lda = K;
+        g.B = m->d_w16 + L.w16_off[l];
+        g.strideB = W;
+        g.ldb = K;
+        g.M = rows;
+        g.N = N;
+        g.K = K;
+        g.bias = m->d_p + L.b_off[l];
+        g.strideBias = P;
+        g.out = m->d_z[l];
+        g.strideOut = (long long)m->cap * N;
+        g.out2 = m->d_act[l + 1];
+        e = es::gemm<false, false, es::kEpiHidden>(g, m->nets, m->stream);
+        m->launches++;
+    }
+    // the FP32 head
+    if (e == cudaSuccess) {
+        const int last = es::kLayers - 1;
+        es::head_forward_kernel<<<dim3((rows + 7) / 8, m->nets), 256, 0, m->stream>>>(
+            m->d_z[last - 1], m->d_p + L.w_off[last], m->d_p + L.b_off[last], P, rows, m->cap, m->d_z[last]);
+        m->launches++;
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+// Backward pass from the FP32 output gradient in d_dy: the head in FP32, then
+// the trunk's weight and bias gradients into d_g.
+cudaError_t backward(es_mlp* m, int rows)
+{
+    const Layout& L = layout();
+    const long long P = L.n_params, W = L.n_weights;
+    cudaError_t e = cudaSuccess;
+    {
+        const int last = es::kLayers - 1;
+        es::head_backward_w_kernel<<<dim3(1, m->nets), es::kHidden, 0, m->stream>>>(
+            m->d_dy, m->d_z[last - 1], rows, m->cap, m->d_g + L.w_off[last], m->d_g + L.b_off[last], P);
+        m->launches++;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        const long long n = (long long)rows * es::kHidden;
+        es::head_backward_dz_kernel<<<dim3((unsigned)((n + 255) / 256), m->nets), 256, 0, m->stream>>>(
+            m->d_dy, m->d_z[last - 1], m->d_p + L.w_off[last], P, rows, m->cap, m->d_dz[last - 1]);
+        m->launches++;
+        e = cudaGetLastError();
+    }
+    for (int l = es::kLayers - 2; l >= 0 && e == cudaSuccess; l--) {
+        const int K = es::kDims[l], N = es::kDims[l + 1];
+        // dW_l[n][k] = sum_m dZ_l[m][n] A_l[m][k]
+        es::GemmArgs gw = args0();
+        gw.A = m->d_dz[l];
+        gw.strideA = (long long)m->cap * N;
+        gw.lda = N;
+        gw.B = m->d_act[l];
+        gw.strideB = (long long)m->cap * K;
+        gw.ldb = K;
+        gw.M = N;
+        gw.N = K;
+        gw.K = rows;
+        gw.out = m->d_g + L.w_off[l];
+        gw.strideOut = P;
+        // gemm writes out[n * K + k] with row stride = gw.N = K
+        e = es::gemm<true, true, es::kEpiPlain>(gw, m->nets, m->stream);
+        m->launches++;
+        if (e != cudaSuccess) break;
+        es::bias_grad_kernel<<<dim3((N + 255) / 256, m->nets), 256, 0, m->stream>>>(m->d_dz[l], rows, m->cap, N,
+                                                                                     m->d_g + L.b_off[l], P);
+        m->launches++;
+        if ((e = cudaGetLastError()) != cudaSuccess) break;
+        if (l == 0) break;
+        // dZ_{l-1}[m][k] = (sum_n dZ_l[m][n] W_l[n][k]) * GELU'(Z_{l-1}[m][k])
+        es::GemmArgs gx = args0();
+        gx.A = m->d_dz[l];
+        gx.strideA = (long long)m->cap * N;
+        gx.lda = N;
+        gx.B = m->d_w16 + L.w16_off[l];
+        gx.strideB = W;
+        gx.ldb = K;
+        gx.M = rows;
+        gx.N = K;
+        gx.K = N;
+        gx.out2 = m->d_dz[l - 1];
+        gx.strideOut = (long long)m->cap * K;
+        gx.zprev = m->d_z[l - 1];
+        e = es::gemm<false, true, es::kEpiDGelu>(gx, m->nets, m->stream);
+        m->launches++;
+    }
+    return e;
+}
+
+es_status bind_mlp(es_mlp* m)
+{
+    if (!m) return ES_ERR_BAD_ARG;
+    ES_MCUDA(cudaSetDevice(m->device), "cudaSetDevice");
+    return ES_OK;
+}
+
+// Loss and gradients on the staged minibatch (d_act[0], d_yb).
+es_status loss_and_grads(es_mlp* m, int rows)
+{
+    cudaError_t e = forward(m, rows, false);
+    if (e == cudaSuccess) {
+        es::loss_kernel<<<m->nets, 256, 0, m->stream>>>(m->d_z[es::kLayers - 1], m->d_yb, rows, m->cap, m->d_dy,
+                                                        m->d_loss);
+        m->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = backward(m, rows);
+    ES_MCUDA(e, "surrogate training step");
+    return ES_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t es_mlp_param_count(void) { return layout().n_params; }
+
+es_status es_mlp_create(int32_t n_nets, int32_t device_ordinal, es_mlp** out)
+{
+    if (!out || n_nets < 1 || n_nets > 64) return ES_ERR_BAD_ARG;
+    *out = nullptr;
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device_ordinal < 0 || device_ordinal >= n_dev) {
+        es::set_global_error("es_mlp_create: no such CUDA device");
+        return ES_ERR_DEVICE;
+    }
+    es_mlp* m = new (std::nothrow) es_mlp();
+    if (!m) return ES_ERR_OOM;
+    m->device = device_ordinal;
+    m->nets = n_nets;
+    const Layout& L = layout();
+    const long long P = L.n_params * n_nets, W = L.n_weights * n_nets;
+    std::vector<int> is_w((size_t)P, -1);
+    for (int k = 0; k < n_nets; k++)
+        for (int l = 0; l < es::kLayers; l++) {
+            const long long nk = (long long)es::kDims[l] * es::kDims[l + 1];
+            for (long long i = 0; i < nk; i++)
+                is_w[(size_t)(k * L.n_params + L.w_off[l] + i)] = (int)(k * L.n_weights + L.w16_off[l] + i);
+        }
+    cudaError_t e = cudaSetDevice(device_ordinal);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_p, sizeof(float) * P);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_g, sizeof(float) * P);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_m1, sizeof(float) * P);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_m2, sizeof(float) * P);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_w16, sizeof(__nv_bfloat16) * W);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_is_weight, sizeof(int) * P);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_loss, sizeof(float) * n_nets);
+    if (e == cudaSuccess) e = cudaMallocHost(&m->h_loss, sizeof(float) * n_nets);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(m->d_is_weight, is_w.data(), sizeof(int) * P, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(m->d_p, 0, sizeof(float) * P);
+    if (e == cudaSuccess) e = cudaMemset(m->d_m1, 0, sizeof(float) * P);
+    if (e == cudaSuccess) e = cudaMemset(m->d_m2, 0, sizeof(float) * P);
+    if (e == cudaSuccess) e = cudaMemset(m->d_w16, 0, sizeof(__nv_bfloat16) * W);
+    if (e != cudaSuccess) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "es_mlp_create: %s", cudaGetErrorString(e));
+        es::set_global_error(msg);
+        es_mlp_destroy(m);
+        return e == cudaErrorMemoryAllocation ? ES_ERR_OOM : ES_ERR_LAUNCH;
+    }
+    *out = m;
+    return ES_OK;
+}
+
+es_status es_mlp_destroy(es_mlp* m)
+{
+    if (!m) return ES_ERR_BAD_ARG;
+    cudaSetDevice(m->device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    free_work(m);
+    cudaFree(m->d_p);
+    cudaFree(m->d_g);
+    cudaFree(m->d_m1);
+    cudaFree(m->d_m2);
+    cudaFree(m->d_w16);
+    cudaFree(m->d_is_weight);
+    cudaFree(m->d_x);
+    cudaFree(m->d_y);
+    cudaFree(m->d_loss);
+    if (m->h_loss) cudaFreeHost(m->h_loss);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+    return ES_OK;
+}
+
+const char* es_mlp_last_error(const es_mlp* m) { return m ? m->err : es_last_error(nullptr); }
+
+es_status es_mlp_set_params(es_mlp* m, const float* params)
+{
+    es_status st = bind_mlp(m);
+    if (st != ES_OK) return st;
+    if (!params) return mfail(m, ES_ERR_BAD_ARG, "null parameters");
+    const Layout& L = layout();
+    const long long P = L.n_params * m->nets;
+    ES_MCUDA(cudaMemcpyAsync(m->d_p, params, sizeof(float) * P, cudaMemcpyHostToDevice, m->stream), "parameter upload");
+    ES_MCUDA(cudaMemsetAsync(m->d_m1, 0, sizeof(float) * P, m->stream), "Adam state");
+    ES_MCUDA(cudaMemsetAsync(m->d_m2, 0, sizeof(float) * P, m->stream), "Adam state");
+    for (int k = 0; k < m->nets; k++)
+        for (int l = 0; l < es::kLayers; l++) {
+            const long long nk = (long long)es::kDims[l] * es::kDims[l + 1];
+            es::to_bf16_kernel<<<(unsigned)((nk + 255) / 256), 256, 0, m->stream>>>(
+                m->d_p + k * L.n_params + L.w_off[l], m->d_w16 + k * L.n_weights + L.w16_off[l], nk);
+            m->launches++;
+        }
+    ES_MCUDA(cudaGetLastError(), "weight conversion");
+    ES_MCUDA(cudaStreamSynchronize(m->stream), "parameter upload");
+    m->step = 0;
+    return ES_OK;
+}
+
+es_status es_mlp_get_params(es_mlp* m, float* params)
+{
+    es_status st = bind_mlp(m);
+    if (st != ES_OK) return st;
+    if (!params) return mfail(m, ES_ERR_BAD_ARG, "null parameters");
+    ES_MCUDA(cudaMemcpyAsync(params, m->d_p, sizeof(float) * layout().n_params * m->nets, cudaMemcpyDeviceToHost,
+                             m->stream),
+             "parameter readback");
+    ES_MCUDA(cudaStreamSynchronize(m->stream), "parameter readback");
+    return ES_OK;
+}
+
+es_status es_mlp_set_dataset(es_mlp* m, const float* x, const float* y, int64_t n)
+{
+    es_status st = bind_mlp(m);
+    if (st != ES_OK) return st;
+    if (!x || !y || n < 1) return mfail(m, ES_ERR_BAD_ARG, "empty dataset");
+    cudaFree(m->d_x);
+    cudaFree(m->d_y);
+    m->d_x = m->d_y = nullptr;
+    m->n_data = 0;
+    ES_MCUDA(cudaMalloc(&m->d_x, sizeof(float) * n * es::kIn), "dataset");
+    ES_MCUDA(cudaMalloc(&m->d_y, sizeof(float) * n * es::kOut), "dataset");
+    ES_MCUDA(cudaMemcpyAsync(m->d_x, x, sizeof(float) * n * es::kIn, cudaMemcpyHostToDevice, m->stream), "dataset");
+    ES_MCUDA(cudaMemcpyAsync(m->d_y, y, sizeof(float) * n * es::kOut, cudaMemcpyHostToDevice, m->stream), "dataset");
+    ES_MCUDA(cudaStreamSynchronize(m->stream), "dataset");
+    m->n_data = n;
+    return ES_OK;
+}
+
+es_status es_mlp_train(es_mlp* m, int32_t steps, int32_t batch, float lr, uint64_t seed, float* out_loss)
+{
+    es_status st = bind_mlp(m);
+    if (st != ES_OK) return st;
+    if (m->n_data < 1) return mfail(m, ES_ERR_BAD_ARG, "es_mlp_set_dataset has not been called");
+    if (steps < 0 || batch < 1 || batch > 65536 || !(lr > 0.0f))
+        return mfail(m, ES_ERR_BAD_ARG, "bad training arguments");
+    if ((st = ensure_rows(m, batch)) != ES_OK) return st;
+    const Layout& L = layout();
+    const long long P = L.n_params * m->nets;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (int s = 0; s < steps; s++) {
+        es::gather_kernel<<<dim3((batch + 255) / 256, m->nets), 256, 0, m->stream>>>(
+            m->d_x, m->d_y, m->n_data, batch, m->cap, seed, m->step, m->d_act[0], m->d_yb);
+        m->launches++;
+        ES_MCUDA(cudaGetLastError(), "minibatch gather");
+        if ((st = loss_and_grads(m, batch)) != ES_OK) return st;
+        m->step++;
+        const float c1 = 1.0f - std::pow(b1, (float)m->step), c2 = 1.0f - std::pow(b2, (float)m->step);
+        es::adam_kernel<<<(unsigned)((P + 255) / 256), 256, 0, m->stream>>>(m->d_p, m->d_g, m->d_m1, m->d_m2, m->d_w16,
+                                                                           m->d_is_weight, P, lr, b1, b2, eps, c1, c2);
+        m->launches++;
+        ES_MCUDA(cudaGetLastError(), "Adam update");
+    }
+    if (out_loss) {
+        ES_MCUDA(cudaMemcpyAsync(m->h_loss, m->d_loss, sizeof(float) * m->nets, cudaMemcpyDeviceToHost, m->stream),
+                 "loss readback");
+    }
+    ES_MCUDA(cudaStreamSynchronize(m->stream), "training");
+    if (out_loss) std::memcpy(out_loss, m->h_loss, sizeof(float) * m->nets);
+    return ES_OK;
+}
+
+es_status es_mlp_gradients(es_mlp* m, const float* x, const float* y, int32_t rows, float* out_grads, float* out_loss)
+{
+    es_status st = bind_mlp(m);
+    if (st != ES_OK) return st;
+    if (!x || !y || !out_grads || rows < 1) return mfail(m, ES_ERR_BAD_ARG, "bad gradient arguments");
+    if ((st = ensure_rows(m, rows)) != ES_OK) return st;
+    // x: [nets][rows][kIn] FP32 (rounded to BF16 here), y: [nets][rows][kOut]
+    float* d_tmp = nullptr;
+    const long long nx = (long long)m->nets * rows * es::kIn;
+    ES_MCUDA(cudaMalloc(&d_tmp, sizeof(float) * nx), "gradient input");
+    cudaError_t e = cudaMemcpyAsync(d_tmp, x, sizeof(float) * nx, cudaMemcpyHostToDevice, m->stream);
+    if (e == cudaSuccess) {
+        // rows are packed with stride `rows`; the work buffers use stride `cap`
+        for (int k = 0; k < m->nets && e == cudaSuccess; k++) {
+            es::to_bf16_kernel<<<(unsigned)((rows * es::kIn + 255) / 256), 256, 0, m->stream>>>(
+                d_tmp + (long long)k * rows * es::kIn, m->d_act[0] + (long long)k * m->cap * es::kIn,
+                (long long)rows * es::kIn);
+            m->launches++;
+            e = cudaGetLastError();
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(m->d_yb + (long long)k * m->cap * es::kOut, y + (long long)k * rows * es::kOut,
+                                    sizeof(float) * rows * es::kOut, cudaMemcpyHostToDevice, m->stream);
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    cudaFree(d_tmp);
+    ES_MCUDA(e, "gradient inputs");
+    if ((st = loss_and_grads(m, rows)) != ES_OK) return st;
+    ES_MCUDA(cudaMemcpyAsync(out_grads, m->d_g, sizeof(float) * layout().n_params * m->nets, cudaMemcpyDeviceToHost,
+                             m->stream),
+             "gradient readback");
+    ES_MCUDA(cudaMemcpyAsync(m->h_loss, m->d_loss, sizeof(float) * m->nets, cudaMemcpyDeviceToHost, m->stream),
+             "loss readback");
+    ES_MCUDA(cudaStreamSynchronize(m->stream), "gradients");
+    if (out_loss) std::memcpy(out_loss, m->h_loss, sizeof(float) * m->nets);
+    return ES_OK;
+}
+
+es_status es_mlp_predict(es_mlp* m, const float* x, int64_t q, float* out_each, float* out_mean, float* out_spread)
+{
+    es_status st = bind_mlp(m);
+    if (st != ES_OK) return st;
+    if (!x || q < 1) return mfail(m, ES_ERR_BAD_ARG, "bad query arguments");
+    if ((st = ensure_rows(m, q)) != ES_OK) return st;
+    cudaError_t e = cudaMemcpyAsync(m->d_xin, x, sizeof(float) * q * es::kIn, cudaMemcpyHostToDevice, m->stream);
+    if (e == cudaSuccess) {
+        es::to_bf16_kernel<<<(unsigned)((q * es::kIn + 255) / 256), 256, 0, m->stream>>>(m->d_xin, m->d_act[0],
+                                                                                         q * es::kIn);
+        m->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = forward(m, (int)q, true);
+    if (e == cudaSuccess) {
+        // outputs of member k are at d_z[last] + k * cap * kOut; pack them with stride q
+        if (m->cap != q) {
+            for (int k = 0; k < m->nets && e == cudaSuccess; k++)
+                e = cudaMemcpyAsync(m->d_yb + (long long)k * q * es::kOut,
+                                    m->d_z[es::kLayers - 1] + (long long)k * m->cap * es::kOut,
+                                    sizeof(float) * q * es::kOut, cudaMemcpyDeviceToDevice, m->stream);
+        } else {
+            e = cudaMemcpyAsync(m->d_yb, m->d_z[es::kLayers - 1], sizeof(float) * m->nets * q * es::kOut,
+                                cudaMemcpyDeviceToDevice, m->stream);
+        }
+    }
+    if (e == cudaSuccess) {
+        es::ensemble_kernel<<<(unsigned)((q * es::kOut + 255) / 256), 256, 0, m->stream>>>(m->d_yb, m->nets, q,
+                                                                                           m->d_mean, m->d_spread);
+        m->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && out_each)
+        e = cudaMemcpyAsync(out_each, m->d_yb, sizeof(float) * m->nets * q * es::kOut, cudaMemcpyDeviceToHost,
+                            m->stream);
+    if (e == cudaSuccess && out_mean)
+        e = cudaMemcpyAsync(out_mean, m->d_mean, sizeof(float) * q * es::kOut, cudaMemcpyDeviceToHost, m->stream);
+    if (e == cudaSuccess && out_spread)
+        e = cudaMemcpyAsync(out_spread, m->d_spread, sizeof(float) * q * es::kOut, cudaMemcpyDeviceToHost, m->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    ES_MCUDA(e, "surrogate query");
+    return ES_OK;
+}
+
+int64_t es_mlp_launch_count(const es_mlp* m) { return m ? m->launches : 0; }
+
+void* es_mlp_stream(es_mlp* m) { return m ? (void*)m->stream : nullptr; }
+
+}  // extern "C"

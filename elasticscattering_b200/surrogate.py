@@ -1,0 +1,310 @@
+"""Learned surrogate for sigma(B, T, density, impurity radius, tau), with fallback.
+
+No reference counterpart. An ensemble of four MLPs (es_mlp_* in
+include/es_cuda.h: 5 -> 256 x 4 -> 2, GELU, BF16 weights, FP32 accumulation,
+trained on the GPU by the library's own forward and backward kernels) answers
+sigma queries; wherever the members disagree by more than the tolerance (their
+standard deviation over |mean|, per output), the query is answered by the
+simulator instead -- the batched split-precision path, which also generates the
+training data and judges the surrogate's error.
+
+Features (each mapped onto about [-1, 1]): log B, T, log density, impurity
+radius, log tau. Targets: the total sigma (coherent + incoherent sector, as the
+reference's results combine them) divided by the Drude scale
+sigma_0 = SigmaFactor(tau) at omega = 0 (src/sim/Simulation.h:69-76), so both
+outputs are of order one.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .workloads import E_CHARGE, M_EFF, T_ZERO_STANDIN, orbit_diameter
+
+# src/sim/es/constants.h:23-38
+HBAR = 1.05457148e-34
+C1 = 1.15e-9
+
+# feature ranges of the training distribution (config 4)
+B_RANGE = (0.5, 50.0)
+T_RANGE = (0.0, 40.0)
+N_RANGE = (5e14, 2e16)
+TAU_RANGE = (1e-13, 1e-11)
+R_SCALE = 2e-9
+
+
+def sigma0(tau, speed: float = 1.68e5):
+    """SigmaFactor at omega = 0 with the 1e-8 scale of GetSigmaIntegrandFactor
+    (src/sim/Simulation.h:69-76,88): e^2 k_F^2 tau / (2 pi^2 m* C1) * 1e-8."""
+    kf = M_EFF * speed / HBAR
+    return (E_CHARGE ** 2 * kf ** 2) / (2.0 * math.pi ** 2 * M_EFF * C1) * np.asarray(tau) * 1e-8
+
+
+def features(q: np.ndarray) -> np.ndarray:
+    """q [n][5] = (B, T, density, impurity radius, tau) -> normalised features."""
+    q = np.asarray(q, dtype=np.float64)
+
+    def logmap(v, lo, hi):
+        return 2.0 * (np.log(v) - math.log(lo)) / (math.log(hi) - math.log(lo)) - 1.0
+
+    f = np.empty((len(q), 5))
+    f[:, 0] = logmap(q[:, 0], *B_RANGE)
+    f[:, 1] = 2.0 * (q[:, 1] - T_RANGE[0]) / (T_RANGE[1] - T_RANGE[0]) - 1.0
+    f[:, 2] = logmap(q[:, 2], *N_RANGE)
+    f[:, 3] = q[:, 3] / R_SCALE - 1.0
+    f[:, 4] = logmap(q[:, 4], *TAU_RANGE)
+    return f.astype(np.float32)
+
+
+def drude(q: np.ndarray) -> np.ndarray:
+    """Drude shape of sigma / sigma_0 at the query's tau: (1, w tau) / (1 + (w tau)^2),
+    w = e B / m* (src/sim/SimulationCPU.cpp:107)."""
+    q = np.asarray(q, dtype=np.float64)
+    wt = E_CHARGE * q[:, 0] / M_EFF * q[:, 4]
+    d = 1.0 + wt * wt
+    return np.stack([1.0 / d, wt / d], axis=1)
+
+
+def targets(q: np.ndarray, sigma: np.ndarray) -> np.ndarray:
+    """sigma -> network targets: log(sigma / (sigma_0 * Drude shape)), the impurity
+    and temperature correction to the Drude form. An absolute error in a target
+    is the relative error in sigma, and the targets stay of order one although
+    sigma / sigma_0 spans four decades (w tau from ~2e-3 to ~140)."""
+    q = np.asarray(q, dtype=np.float64)
+    r = np.asarray(sigma, dtype=np.float64) / (sigma0(q[:, 4])[:, None] * drude(q))
+    if not (r > 0).all():
+        raise ValueError("surrogate targets need sigma_xx, sigma_xy > 0 (clockwise carriers)")
+    return np.log(r).astype(np.float32)
+
+
+def untarget(q: np.ndarray, t: np.ndarray) -> np.ndarray:
+    """Inverse of targets(); t [..., n, 2]."""
+    q = np.asarray(q, dtype=np.float64)
+    return np.exp(np.asarray(t, dtype=np.float64)) * sigma0(q[:, 4])[:, None] * drude(q)
+
+
+def init_params(n_nets: int, seed: int) -> np.ndarray:
+    """He-uniform weights for GELU layers, zero biases; one block per member."""
+    from math import sqrt
+    rng = np.random.default_rng(seed)
+    dims = (5, 256, 256, 256, 256, 2)
+    out = []
+    for _ in range(n_nets):
+        for k, n in zip(dims[:-1], dims[1:]):
+            lim = sqrt(6.0 / k) if n != dims[-1] else sqrt(3.0 / k)
+            out.append(rng.uniform(-lim, lim, size=n * k))
+            out.append(np.zeros(n))
+    return np.concatenate(out).astype(np.float32)
+
+
+class MLPEnsemble:
+    """Owner of one es_mlp."""
+
+    def __init__(self, n_nets: int = 4, device: int = 0):
+        h = C.c_void_p()
+        st = N.cuda_lib().es_mlp_create(int(n_nets), int(device), C.byref(h))
+        if st != N.ES_OK:
+            N.check(st, None)
+        self._m = h
+        self.n_nets = int(n_nets)
+        self.P = int(N.cuda_lib().es_mlp_param_count())
+
+    def close(self) -> None:
+        if getattr(self, "_m", None) and self._m.value:
+            N.cuda_lib().es_mlp_destroy(self._m)
+            self._m = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int) -> None:
+        N.check_mlp(st, self._m)
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.n_nets * self.P
+        self._check(N.cuda_lib().es_mlp_set_params(self._m, p.ctypes.data))
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.n_nets * self.P, dtype=np.float32)
+        self._check(N.cuda_lib().es_mlp_get_params(self._m, p.ctypes.data))
+        return p
+
+    def set_dataset(self, x: np.ndarray, y: np.ndarray) -> None:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        self._check(N.cuda_lib().es_mlp_set_dataset(self._m, x.ctypes.data, y.ctypes.data, len(x)))
+
+    def train(self, steps: int, batch: int, lr: float, seed: int = 0) -> np.ndarray:
+        loss = np.zeros(self.n_nets, dtype=np.float32)
+        self._check(N.cuda_lib().es_mlp_train(self._m, int(steps), int(batch), float(lr), int(seed) & (2**64 - 1),
+                                              loss.ctypes.data))
+        return loss
+
+    def gradients(self, x: np.ndarray, y: np.ndarray):
+        """x [n_nets][rows][5], y [n_nets][rows][2] -> (grads [n_nets][P], loss [n_nets])."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        rows = x.shape[1]
+        g = np.zeros(self.n_nets * self.P, dtype=np.float32)
+        loss = np.zeros(self.n_nets, dtype=np.float32)
+        self._check(N.cuda_lib().es_mlp_gradients(self._m, x.ctypes.data, y.ctypes.data, rows, g.ctypes.data,
+                                                  loss.ctypes.data))
+        return g.reshape(self.n_nets, self.P), loss
+
+    def predict(self, x: np.ndarray):
+        """x [q][5] -> (each [n_nets][q][2], mean [q][2], spread [q][2])."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        q = len(x)
+        each = np.zeros((self.n_nets, q, 2), dtype=np.float32)
+        mean = np.zeros((q, 2), dtype=np.float32)
+        spread = np.zeros((q, 2), dtype=np.float32)
+        self._check(N.cuda_lib().es_mlp_predict(self._m, x.ctypes.data, q, each.ctypes.data, mean.ctypes.data,
+                                                spread.ctypes.data))
+        return each, mean, spread
+
+    def launch_count(self) -> int:
+        return int(N.cuda_lib().es_mlp_launch_count(self._m))
+
+
+@dataclass
+class Resolution:
+    """Simulator resolution used for training data and fallback answers."""
+    dim: int = 65
+    phi_steps: int = 25
+    region_size: float = 1e-6
+    b_min: float = B_RANGE[0]     # sets region_extends (one orbit diameter at b_min)
+    density_levels: int = 16      # densities are snapped to this many log-spaced levels
+    target_cell_population: int = 12
+    seed: int = 100               # Grid seed: one impurity stream for every density
+    particle_speed: float = 1.68e5
+    alpha: float = 0.3
+
+
+class Simulator:
+    """sigma for query rows (B, T, density, impurity radius, tau) from the batched
+    split-precision path: per query one coherent and one incoherent pass, their
+    sigma added. Densities are snapped to log-spaced levels so that grids (one
+    per level, built once) are shared; every grid uses the same seed and
+    extends, so a higher density adds impurities to a lower one's."""
+
+    def __init__(self, res: Resolution | None = None, device: int = 0):
+        from .batch import BatchSweep
+        self.res = res or Resolution()
+        self.device = device
+        self.levels = np.exp(np.linspace(math.log(N_RANGE[0]), math.log(N_RANGE[1]), self.res.density_levels))
+        self.grids = {}
+        self.batch = BatchSweep(device)
+        self.grid_ids = {}
+
+    def close(self) -> None:
+        self.batch.close()
+
+    def snap(self, density):
+        idx = np.abs(np.log(np.asarray(density))[:, None] - np.log(self.levels)[None, :]).argmin(axis=1)
+        return idx
+
+    def _grid(self, density: float, radius: float):
+        from .simulation import Grid
+        key = (float(density), float(radius))
+        if key not in self.grids:
+            r = self.res
+            g = Grid.from_seed(r.seed, r.region_size, orbit_diameter(r.particle_speed, r.b_min), float(density),
+                               float(radius), r.target_cell_population, max_impurities=1 << 31)
+            self.grids[key] = g
+            self.grid_ids[key] = self.batch.add_grid(g)
+        return self.grids[key], self.grid_ids[key]
+
+    def snapped(self, q: np.ndarray) -> np.ndarray:
+        """The query rows with their density replaced by the nearest level."""
+        q = np.array(q, dtype=np.float64)
+        q[:, 2] = self.levels[self.snap(q[:, 2])]
+        return q
+
+    def __call__(self, q: np.ndarray) -> np.ndarray:
+        """sigma [n][2] at exactly the queried densities (one grid per distinct density)."""
+        from .batch import BatchPass
+        from .simulation import make_settings
+        q = np.asarray(q, dtype=np.float64)
+        r = self.res
+        ext = orbit_diameter(r.particle_speed, r.b_min)
+        passes = []
+        for k, (B, T, dens, rad, tau) in enumerate(q):
+            g, gid = self._grid(dens, rad)
+            st = make_settings(float(tau), r.alpha, True, r.particle_speed, r.region_size, ext, float(dens),
+                               float(rad), r.target_cell_population)
+            t_inc = float(T) if T > 0 else T_ZERO_STANDIN
+            for coherent in (True, False):
+                passes.append(BatchPass(gid, r.dim, r.phi_steps, coherent, r.region_size, g.info().cell_size,
+                                        float(B), st, [t_inc]))
+        self.batch.set_passes(passes)
+        out, _ = self.batch.run(with_metrics=False)
+        s = out[:, 0, :]
+        return s[0::2] + s[1::2]
+
+
+def sample_queries(n: int, seed: int, b_range=B_RANGE, n_range=N_RANGE, tau_range=TAU_RANGE,
+                   t_range=T_RANGE, radius: float = R_SCALE) -> np.ndarray:
+    """Config-4 draws: B, density and tau log-uniform, T uniform, radius fixed."""
+    rng = np.random.default_rng(seed)
+
+    def logu(lo, hi, size):
+        return np.exp(rng.uniform(math.log(lo), math.log(hi), size))
+
+    q = np.empty((n, 5))
+    q[:, 0] = logu(*b_range, n)
+    q[:, 1] = rng.uniform(*t_range, n)
+    q[:, 2] = logu(*n_range, n)
+    q[:, 3] = radius
+    q[:, 4] = logu(*tau_range, n)
+    return q
+
+
+class Surrogate:
+    """Ensemble + simulator fallback: answers sigma queries within `tolerance`."""
+
+    def __init__(self, ensemble: MLPEnsemble, simulator: Simulator, tolerance: float = 0.01):
+        self.ens = ensemble
+        self.sim = simulator
+        self.tolerance = tolerance
+
+    def fit(self, q: np.ndarray, sigma: np.ndarray, steps: int = 4000, batch: int = 256, lr: float = 1e-3,
+            seed: int = 0, lr_decay_rounds: int = 4) -> list:
+        """Trains every member on (features(q), sigma / sigma_0); the learning
+        rate halves after each of `lr_decay_rounds` equal rounds."""
+        self.ens.set_params(init_params(self.ens.n_nets, seed))
+        self.ens.set_dataset(features(q), targets(q, sigma))
+        losses = []
+        per = max(1, steps // lr_decay_rounds)
+        for k in range(lr_decay_rounds):
+            losses.append(self.ens.train(per, batch, lr * 0.5 ** k, seed=seed + 7 * k).tolist())
+        return losses
+
+    def query(self, q: np.ndarray):
+        """-> (sigma [n][2], fell_back [n] bool, spread [n], timings dict)."""
+        q = np.asarray(q, dtype=np.float64)
+        t0 = time.perf_counter()
+        each, _, _ = self.ens.predict(features(q))
+        members = untarget(q, each)                     # [n_nets][n][2] sigma
+        sig = members.mean(axis=0)
+        spread = members.std(axis=0) / np.maximum(np.abs(sig), 1e-300)
+        t_nn = time.perf_counter() - t0
+        worst = spread.max(axis=1)
+        fb = worst > self.tolerance
+        t_fb = 0.0
+        if fb.any():
+            t1 = time.perf_counter()
+            sig[fb] = self.sim(q[fb])
+            t_fb = time.perf_counter() - t1
+        return sig, fb, worst, {"network_s": t_nn, "fallback_s": t_fb}

@@ -320,6 +320,45 @@ int64_t es_batch_launch_count(const es_batch* b);
 /* Orbits per run of the current instance table. */
 int64_t es_batch_total_orbits(const es_batch* b);
 
+/* ---------------------------------------------------------------------------
+ * Learned surrogate. No reference counterpart: an ensemble of MLPs,
+ * 5 -> 256 x 4 -> 2 with GELU; the hidden layers in BF16 weights and
+ * activations with FP32 accumulation on the tensor cores, the 256 -> 2 head in
+ * FP32; trained on the GPU by this library's own forward and backward kernels. Inputs are 5 normalised features per query, outputs 2
+ * normalised targets per query and member; the normalisation and the fallback
+ * to the simulator live with the caller.
+ * Parameter layout of one member: for each of the 5 layers, W [N][K] row-major
+ * then b [N], with (K, N) = (5, 256), (256, 256) x 3, (256, 2); members follow
+ * each other.
+ * ------------------------------------------------------------------------- */
+
+typedef struct es_mlp es_mlp;
+
+/* Parameters of one member (199,426). */
+int64_t es_mlp_param_count(void);
+es_status es_mlp_create(int32_t n_nets, int32_t device_ordinal, es_mlp** out);
+es_status es_mlp_destroy(es_mlp* m);
+const char* es_mlp_last_error(const es_mlp* m);
+/* FP32 parameters of every member (n_nets * es_mlp_param_count() floats); resets Adam. */
+es_status es_mlp_set_params(es_mlp* m, const float* params);
+es_status es_mlp_get_params(es_mlp* m, float* params);
+/* Training set: x [n][5], y [n][2] (host, FP32), copied to the device. */
+es_status es_mlp_set_dataset(es_mlp* m, const float* x, const float* y, int64_t n);
+/* `steps` Adam steps (beta 0.9 / 0.999, eps 1e-8) of every member on its own
+ * bootstrap minibatches of `batch` rows (drawn from `seed` and the step count);
+ * out_loss (n_nets floats, may be NULL) receives the last step's mean squared error. */
+es_status es_mlp_train(es_mlp* m, int32_t steps, int32_t batch, float lr, uint64_t seed, float* out_loss);
+/* Loss and gradients without an update, for checking: x [n_nets][rows][5],
+ * y [n_nets][rows][2]; out_grads n_nets * es_mlp_param_count() floats. */
+es_status es_mlp_gradients(es_mlp* m, const float* x, const float* y, int32_t rows, float* out_grads,
+                           float* out_loss);
+/* Every member on the same q queries x [q][5]: out_each [n_nets][q][2], out_mean
+ * [q][2], out_spread [q][2] (ensemble standard deviation / |mean|); any output
+ * pointer may be NULL. */
+es_status es_mlp_predict(es_mlp* m, const float* x, int64_t q, float* out_each, float* out_mean, float* out_spread);
+int64_t es_mlp_launch_count(const es_mlp* m);
+void* es_mlp_stream(es_mlp* m);
+
 /* Measured FP64 FMA throughput of a device (TFLOP/s, 2 FLOP per FMA): the
  * denominator of the lifetime kernel's roofline. No reference counterpart
  * (the reference publishes no device figures). Runs for a few milliseconds. */

@@ -1,0 +1,138 @@
+"""The learned surrogate's GPU kernels (es_mlp_*) against the FP64 checker, and
+the surrogate with fallback against the simulator it stands in for.
+
+- forward pass of every ensemble member vs oracle/mlp_ref.py (same BF16
+  roundings, FP64 elsewhere): within 2e-3 relative (norm);
+- loss and every parameter gradient vs the checker: loss within 1e-3, each
+  weight and bias gradient within 2e-2 relative (norm) -- the residue is the
+  GPU's FP32 accumulation and GELU, and the BF16 roundings they occasionally flip;
+- training drives the loss down and is bit-reproducible;
+- end to end on a reduced physics range: trained on simulator sweeps, the
+  surrogate answers held-out queries within the 1% tolerance where it answers
+  (and hands the rest to the simulator), much faster than the simulator.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import pytest
+
+import mlp_ref
+from elasticscattering_b200 import surrogate as S
+
+pytestmark = pytest.mark.gpu
+
+FWD_RTOL = 2e-3
+LOSS_RTOL = 1e-3
+GRAD_RTOL = 2e-2
+
+
+def member(params: np.ndarray, k: int) -> np.ndarray:
+    P = mlp_ref.param_count()
+    return params[k * P:(k + 1) * P].astype(np.float64)
+
+
+def randomized_params(seed: int) -> np.ndarray:
+    """He-uniform weights plus non-zero biases, so every term is exercised."""
+    p = S.init_params(4, seed)
+    rng = np.random.default_rng(seed + 1)
+    P = mlp_ref.param_count()
+    for k in range(4):
+        o = k * P
+        for kk, n in zip(mlp_ref.DIMS[:-1], mlp_ref.DIMS[1:]):
+            o += kk * n
+            p[o:o + n] = rng.uniform(-0.2, 0.2, size=n)
+            o += n
+    return p
+
+
+def test_forward_matches_fp64_checker(cuda_device):
+    p = randomized_params(11)
+    x = np.random.default_rng(2).uniform(-1, 1, size=(300, 5)).astype(np.float32)
+    with S.MLPEnsemble(4, cuda_device) as ens:
+        ens.set_params(p)
+        each, mean, spread = ens.predict(x)
+    for k in range(4):
+        ref, _ = mlp_ref.forward(member(p, k), x)
+        err = np.linalg.norm(each[k] - ref) / np.linalg.norm(ref)
+        assert err <= FWD_RTOL, (k, err)
+    assert np.allclose(mean, each.mean(axis=0), rtol=1e-5, atol=1e-6)
+    assert np.allclose(spread, each.std(axis=0) / np.abs(each.mean(axis=0)), rtol=1e-3, atol=1e-6)
+
+
+def test_gradients_match_fp64_checker(cuda_device):
+    p = randomized_params(21)
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-1, 1, size=(4, 200, 5)).astype(np.float32)
+    y = rng.uniform(-1, 1, size=(4, 200, 2)).astype(np.float32)
+    with S.MLPEnsemble(4, cuda_device) as ens:
+        ens.set_params(p)
+        grads, loss = ens.gradients(x, y)
+    dims = mlp_ref.DIMS
+    for k in range(4):
+        l_ref, g_ref = mlp_ref.loss_and_grads(member(p, k), x[k], y[k])
+        assert abs(loss[k] - l_ref) <= LOSS_RTOL * l_ref, (k, loss[k], l_ref)
+        o = 0
+        for li, (kk, n) in enumerate(zip(dims[:-1], dims[1:])):
+            for name, size in (("W", kk * n), ("b", n)):
+                a, b = grads[k, o:o + size], g_ref[o:o + size]
+                err = np.linalg.norm(a - b) / np.linalg.norm(b)
+                assert err <= GRAD_RTOL, (k, li, name, err)
+                o += size
+
+
+def test_training_fits_and_is_reproducible(cuda_device):
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-1, 1, size=(4000, 5)).astype(np.float32)
+    y = np.stack([np.sin(2 * x[:, 0]) * np.cos(x[:, 1]) + 0.3 * x[:, 2], x[:, 3] * x[:, 4] - 0.2 * x[:, 0] ** 2],
+                 axis=1).astype(np.float32)
+    runs = []
+    for _ in range(2):
+        with S.MLPEnsemble(4, cuda_device) as ens:
+            ens.set_params(S.init_params(4, 5))
+            ens.set_dataset(x, y)
+            first = ens.train(1, 256, 2e-3, seed=9)
+            last = ens.train(1500, 256, 2e-3, seed=9)
+            runs.append((first, last, ens.get_params()))
+    (f0, l0, p0), (f1, l1, p1) = runs
+    assert (l0 < 0.05 * f0).all(), (f0, l0)
+    assert np.array_equal(p0.view(np.uint32), p1.view(np.uint32))
+    assert np.array_equal(l0, l1)
+
+
+def test_surrogate_answers_within_tolerance_or_falls_back(cuda_device):
+    """Reduced physics range (B 4-40 T, density 5e14-3e15 m^-2; the simulator at
+    65^2 starts x 100 phases): 4000 simulator queries train the ensemble; on 200
+    held-out queries the network answers where its members agree to 1% -- those
+    answers are within 1% of the simulator (95th percentile; 3% at most) -- the
+    rest fall back to the simulator, and the network answers a batch far faster
+    than the simulator does."""
+    res = S.Resolution(dim=65, phi_steps=25, b_min=4.0, density_levels=6)
+    sim = S.Simulator(res, device=cuda_device)
+    try:
+        kw = dict(b_range=(4.0, 40.0), n_range=(5e14, 3e15))
+        sim.levels = np.exp(np.linspace(np.log(5e14), np.log(3e15), res.density_levels))
+        train_q = sim.snapped(S.sample_queries(4000, seed=1, **kw))
+        train_s = sim(train_q)
+        test_q = sim.snapped(S.sample_queries(200, seed=2, **kw))
+        t0 = time.perf_counter()
+        truth = sim(test_q)
+        t_sim = time.perf_counter() - t0
+        with S.MLPEnsemble(4, cuda_device) as ens:
+            sur = S.Surrogate(ens, sim, tolerance=0.01)
+            sur.fit(train_q, train_s, steps=12000, batch=256, lr=2e-3, seed=0)
+            sur.query(test_q[:8])  # warm-up
+            sig, fb, spread, t = sur.query(test_q)
+        err = (np.abs(sig - truth) / np.abs(truth)).max(axis=1)
+        answered = ~fb
+        assert answered.mean() >= 0.5, answered.mean()
+        # the network's own answers: within the tolerance where its members agree
+        assert np.quantile(err[answered], 0.95) <= 0.01, np.quantile(err[answered], 0.95)
+        assert err[answered].max() <= 0.03, err[answered].max()
+        # fallback answers are the simulator's
+        assert err[fb].max(initial=0.0) <= 1e-9
+        # median latency of a query: the network pass alone when it answers
+        assert t_sim / t["network_s"] >= 20, (t_sim, t)
+    finally:
+        sim.close()
