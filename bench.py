@@ -185,6 +185,11 @@ def run_reference(args) -> None:
     if args.workload == "config2":
         run_reference_batched(args)
         return
+    if args.workload == "config4":
+        print(json.dumps({"impl": "reference", "unavailable": "config 4 is the learned surrogate, which has no "
+                          "reference counterpart; the reference's CPU cost per sigma point is in the config-1 and "
+                          "config-2 lines"}))
+        return
     w = workloads.WORKLOADS[args.workload]()
     procs = os.cpu_count() or 1
     rows = max(1, args.ref_rows)
@@ -728,6 +733,90 @@ def run_batched(args) -> None:
     print(json.dumps(line))
 
 
+def run_surrogate(args) -> None:
+    """Config 4: the learned surrogate. Trains the 4-member ensemble on 20k
+    simulator runs (the batched split path, 65^2 starts x 100 phases), then serves
+    4096-query batches with fallback to the simulator where the members disagree
+    by more than 1%, and compares latency and error with the simulator itself."""
+    import torch
+
+    from elasticscattering_b200 import surrogate as S
+
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and int(os.environ.get("RANK", "0")) != 0:
+        return  # replicas only: the surrogate is served from one GPU
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    res = S.Resolution(dim=65, phi_steps=25, b_min=S.B_RANGE[0], density_levels=16)
+    sim = S.Simulator(res, device=dev)
+    build_s = sim.prebuild(sim.levels)
+    t0 = time.perf_counter()
+    train_q = sim.snapped(S.sample_queries(args.train_points, seed=1))
+    train_s = sim(train_q)
+    data_s = time.perf_counter() - t0
+    ens = S.MLPEnsemble(4, dev)
+    sur = S.Surrogate(ens, sim, tolerance=0.01)
+    t0 = time.perf_counter()
+    losses = sur.fit(train_q, train_s, steps=args.train_steps, batch=256, lr=2e-3, seed=0)
+    train_s_time = time.perf_counter() - t0
+    # fallback threshold: calibrated on held-out simulator answers so that the
+    # network's own answers meet the 1% bar at the 95th percentile
+    cal_q = sim.snapped(S.sample_queries(args.judge_queries * 2, seed=50))
+    tol = sur.calibrate(cal_q, sim(cal_q), target=0.01, quantile=0.95)
+
+    Q = 4096
+    batches = [sim.snapped(S.sample_queries(Q, seed=100 + k)) for k in range(args.steps + args.warmup)]
+    for k in range(args.warmup):
+        sur.query(batches[k])
+    net_ms, fb_frac, served = [], [], 0
+    t_total = 0.0
+    for k in range(args.warmup, args.warmup + args.steps):
+        t0 = time.perf_counter()
+        sig, fb, spread, tm = sur.query(batches[k])
+        t_total += time.perf_counter() - t0
+        net_ms.append(1e3 * tm["network_s"])
+        fb_frac.append(float(fb.mean()))
+        served += Q
+    # the simulator on the same kind of batch: latency and the error judge
+    judge_q = batches[-1][:args.judge_queries]
+    t0 = time.perf_counter()
+    truth = sim(judge_q)
+    sim_s = time.perf_counter() - t0
+    sig, fb, spread, tm = sur.query(judge_q)
+    err = (np.abs(sig - truth) / np.abs(truth)).max(axis=1)
+    ans = ~fb
+    nn_only = (np.abs(S.untarget(judge_q, ens.predict(S.features(judge_q))[0]).mean(axis=0) - truth)
+               / np.abs(truth)).max(axis=1)
+    sim_ms_per_query = 1e3 * sim_s / len(judge_q)
+    line = {
+        "metric": "sigma queries/sec (surrogate with fallback)", "value": served / t_total, "unit": "queries/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (hidden layers) + f32 head",
+        "data": "synthetic: config-4 draws (B, density, tau log-uniform; T uniform), densities at the 16 grid levels",
+        "config": {"workload": "config4-surrogate", "queries_per_batch": Q, "train_points": args.train_points,
+                   "train_steps": args.train_steps, "simulator": "batched split path, 65^2 starts x 100 phases",
+                   "error_target": "1% at the 95th percentile of network answers",
+                   "fallback_spread_threshold": tol},
+        "network_latency_ms_per_batch": {"median": statistics.median(net_ms), "max": max(net_ms)},
+        "median_query_latency_ms": statistics.median(net_ms) if statistics.median(fb_frac) < 0.5 else None,
+        "simulator_latency_ms_per_query": sim_ms_per_query,
+        "simulator_latency_ms_per_batch_extrapolated": sim_ms_per_query * Q,
+        "latency_gain_median": (sim_ms_per_query * Q) / statistics.median(net_ms),
+        "fallback_fraction": {"median": statistics.median(fb_frac), "max": max(fb_frac)},
+        "error_vs_simulator": {"queries": int(len(judge_q)), "answered_by_network": int(ans.sum()),
+                               "p50": float(np.median(err)), "p95": float(np.quantile(err, 0.95)),
+                               "max": float(err.max()),
+                               "network_only_p50": float(np.median(nn_only)),
+                               "network_only_p95": float(np.quantile(nn_only, 0.95)),
+                               "network_only_max": float(nn_only.max())},
+        "training": {"grid_build_s": build_s, "data_s": data_s, "train_s": train_s_time,
+                     "final_loss": losses[-1]},
+        "gpu_launches": ens.launch_count(),
+    }
+    ens.close()
+    sim.close()
+    print(json.dumps(line))
+
+
 def profiled_traffic(name: str):
     """DRAM bytes per launch from a committed ncu summary ("split", "fp64" or a
     file name under profiles/), if present."""
@@ -753,7 +842,10 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["split", "fp64"], default="split")
-    ap.add_argument("--workload", default="config1", choices=sorted(workloads.WORKLOADS) + ["config2"])
+    ap.add_argument("--workload", default="config1", choices=sorted(workloads.WORKLOADS) + ["config2", "config4"])
+    ap.add_argument("--train-points", type=int, default=20000, help="config4: simulator runs for training")
+    ap.add_argument("--train-steps", type=int, default=24000, help="config4: Adam steps")
+    ap.add_argument("--judge-queries", type=int, default=512, help="config4: queries checked against the simulator")
     ap.add_argument("--ref-rows", type=int, default=2, help="start-position rows per CPU process")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--samples", type=int, default=8, help="config2: impurity samples per GPU (64 = the full draw)")
@@ -766,6 +858,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "config2":
         run_batched(args)
+    elif args.workload == "config4":
+        run_surrogate(args)
     else:
         run_ours(args)
 

@@ -211,6 +211,27 @@ class Simulator:
     def close(self) -> None:
         self.batch.close()
 
+    def prebuild(self, densities, radius: float = R_SCALE, threads: int = 0) -> float:
+        """Builds the grids of the given densities on host threads (the host build
+        releases the GIL) and copies them to the device; returns the seconds spent."""
+        import os
+        from concurrent.futures import ThreadPoolExecutor
+        from .simulation import Grid
+        t0 = time.perf_counter()
+        r = self.res
+        todo = [float(d) for d in densities if (float(d), float(radius)) not in self.grids]
+
+        def build(d):
+            return Grid.from_seed(r.seed, r.region_size, orbit_diameter(r.particle_speed, r.b_min), d, float(radius),
+                                  r.target_cell_population, max_impurities=1 << 31)
+
+        with ThreadPoolExecutor(max_workers=threads or min(16, os.cpu_count() or 1)) as ex:
+            for d, g in zip(todo, ex.map(build, todo)):
+                key = (d, float(radius))
+                self.grids[key] = g
+                self.grid_ids[key] = self.batch.add_grid(g)
+        return time.perf_counter() - t0
+
     def snap(self, density):
         idx = np.abs(np.log(np.asarray(density))[:, None] - np.log(self.levels)[None, :]).argmin(axis=1)
         return idx
@@ -290,6 +311,24 @@ class Surrogate:
         for k in range(lr_decay_rounds):
             losses.append(self.ens.train(per, batch, lr * 0.5 ** k, seed=seed + 7 * k).tolist())
         return losses
+
+    def calibrate(self, q: np.ndarray, sigma: np.ndarray, target: float = 0.01, quantile: float = 0.95) -> float:
+        """Sets the fallback threshold on ensemble spread from held-out simulator
+        answers: the largest threshold whose network-answered queries have their
+        `quantile` relative error within `target`. Returns the threshold."""
+        q = np.asarray(q, dtype=np.float64)
+        each, _, _ = self.ens.predict(features(q))
+        members = untarget(q, each)
+        mean = members.mean(axis=0)
+        spread = (members.std(axis=0) / np.maximum(np.abs(mean), 1e-300)).max(axis=1)
+        err = (np.abs(mean - sigma) / np.abs(sigma)).max(axis=1)
+        order = np.argsort(spread)
+        best = 0.0
+        for n in range(8, len(order) + 1):
+            if np.quantile(err[order[:n]], quantile) <= target:
+                best = float(spread[order[n - 1]])
+        self.tolerance = best
+        return best
 
     def query(self, q: np.ndarray):
         """-> (sigma [n][2], fell_back [n] bool, spread [n], timings dict)."""
