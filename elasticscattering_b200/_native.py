@@ -103,6 +103,7 @@ CUDA_API = {
     "es_enqueue_sigmas": (_i32, [_vp, _d, _vp, _i32, _vp]),
     "es_enqueue_lifetimes": (_i32, [_vp, _d]),
     "es_synchronize": (_i32, [_vp]),
+    "es_average_lifetime": (_i32, [_vp, C.POINTER(_d)]),
     "es_read_metrics": (_i32, [_vp, C.POINTER(Metrics), _i32]),
     "es_stream": (_vp, [_vp]),
     "es_launch_count": (_i64, [_vp]),
@@ -152,6 +153,8 @@ HOST_API = {
     "es_grid_seed": (_u32, [_vp]),
     "es_grid_generation": (_u64, [_vp]),
     "es_grid_settings": (None, [_vp, C.POINTER(ImpuritySettings)]),
+    "es_run_config": (_i32, [C.c_char_p, C.c_char_p, _i32, _i32]),
+    "es_config_describe": (_i32, [C.c_char_p, C.c_char_p, _i32]),
     "es_host_last_error": (C.c_char_p, []),
 }
 

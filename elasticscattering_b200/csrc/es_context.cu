@@ -607,6 +607,22 @@ es_status es_enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
     return enqueue_lifetimes(ctx, magnetic_field);
 }
 
+es_status es_average_lifetime(es_ctx* ctx, double* out_average)
+{
+    es_status st = bind(ctx);
+    if (st != ES_OK) return st;
+    if (!out_average) return fail(ctx, ES_ERR_BAD_ARG, "es_average_lifetime: null output");
+    if (!ctx->lifetimes_valid) return fail(ctx, ES_ERR_BAD_ARG, "no resident lifetimes: call es_compute_lifetimes first");
+    ES_CUDA(es::launch_lifetime_sum(ctx->d_lifetimes, ctx->n_orbits, ctx->d_partial, ctx->d_sigma, ctx->stream),
+            "lifetime sum");
+    ctx->launches += 2;
+    ES_CUDA(cudaMemcpyAsync(ctx->h_sigma, ctx->d_sigma, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+            "lifetime sum readback");
+    ES_CUDA(cudaStreamSynchronize(ctx->stream), "lifetime sum");
+    *out_average = ctx->h_sigma[0] / (double)ctx->n_orbits;  // Simulation::AverageLifetime
+    return ES_OK;
+}
+
 es_status es_synchronize(es_ctx* ctx)
 {
     es_status st = bind(ctx);

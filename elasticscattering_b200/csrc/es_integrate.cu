@@ -146,6 +146,38 @@ __global__ void __launch_bounds__(256) reduce_partials_kernel(IntegrateLaunch P)
     }
 }
 
+// Sum of the raw lifetimes (Simulation::AverageLifetime's numerator,
+// src/sim/Simulation.h:93-106): kIntegrateBlocks grid-stride partial sums, then
+// one block adds them in a fixed order.
+__global__ void __launch_bounds__(256) lifetime_sum_kernel(const double* lt, long long n, double* partial)
+{
+    __shared__ double s[256];
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        acc += lt[i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
+}
+
+__global__ void __launch_bounds__(256) sum_partials_kernel(const double* partial, int n, double* out)
+{
+    __shared__ double s[256];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
 template <int NT>
 cudaError_t launch_group(const IntegrateLaunch& L, cudaStream_t s)
 {
@@ -171,6 +203,15 @@ cudaError_t launch_integrate(const IntegrateLaunch& L, cudaStream_t s)
     }
     if (e != cudaSuccess) return e;
     reduce_partials_kernel<<<1, 256, 0, s>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lifetime_sum(const double* lifetimes, long long n, double* partial, double* out, cudaStream_t s)
+{
+    lifetime_sum_kernel<<<kIntegrateBlocks, 256, 0, s>>>(lifetimes, n, partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    sum_partials_kernel<<<1, 256, 0, s>>>(partial, kIntegrateBlocks, out);
     return cudaGetLastError();
 }
 

@@ -109,6 +109,8 @@ cudaError_t launch_local_impurities(const double2* imps, const int* cell_end, fl
                                     int cpr, cudaStream_t s);
 // Stages (b)+(c) for one temperature group: two launches.
 cudaError_t launch_integrate(const IntegrateLaunch& L, cudaStream_t s);
+// Sum of n raw lifetimes into *out (device), fixed order; partial holds kIntegrateBlocks doubles.
+cudaError_t launch_lifetime_sum(const double* lifetimes, long long n, double* partial, double* out, cudaStream_t s);
 cudaError_t launch_debug_trace(const LifetimeLaunch& L, const PhaseOrbit& ph, double px, double py, double* d_out,
                                cudaStream_t s);
 cudaError_t launch_debug_next_cell(double cx, double cy, double r, int clockwise, double phi, double start,

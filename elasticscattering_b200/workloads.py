@@ -70,6 +70,10 @@ class Workload:
             lines.append(f"magnetic_field {self.fields[0]!r}")
         else:
             lo, hi = self.fields[0], self.fields[-1]
+            step = (hi - lo) / (len(self.fields) - 1)
+            if any(abs(b - (lo + k * step)) > 1e-12 * max(abs(hi), 1.0) for k, b in enumerate(self.fields)):
+                # src/SimulationConfiguration.h:150-176: one field, or min/max/n uniformly spaced
+                raise ValueError("a .config file holds one magnetic field or a uniformly spaced range")
             lines += [f"magnetic_field_min {lo!r}", f"magnetic_field_max {hi!r}", f"magnetic_field_n {len(self.fields)}"]
         lines += [
             f"particle_speed {self.particle_speed!r}", f"clockwise {1 if self.clockwise else 0}",

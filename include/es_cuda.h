@@ -4,7 +4,7 @@
  * The reference selects a backend behind `class Simulation`
  * (src/sim/Simulation.h:56-147; chosen at src/SimulationRunner.cpp:82-84) and
  * its GPU implementation is an OpenCL context with six kernels
- * (src/sim/SimulationCL.cpp, src/sim/cl/*.cl). This header is the drop-in
+ * (src/sim/SimulationCL.cpp and the .cl files of src/sim/cl). This header is the drop-in
  * replacement for that implementation: plain pointers and sizes, no C++ or
  * framework types. A host wrapper (SimulationCUDA, elasticscattering_b200/host)
  * maps the reference's `Simulation` methods onto these calls one to one.
@@ -176,6 +176,11 @@ es_status es_enqueue_sigmas(es_ctx* ctx, double magnetic_field, const double* te
  * context stream (SimulationCL::ComputeLifetimes without its blocking copies,
  * src/sim/SimulationCL.cpp:113-177). The lifetimes stay resident. */
 es_status es_enqueue_lifetimes(es_ctx* ctx, double magnetic_field);
+
+/* Replaces Simulation::AverageLifetime (src/sim/Simulation.h:93-106): the mean
+ * raw lifetime of the resident pass (the "Avg. particle lifetime" row of
+ * Metrics.txt), summed on the device in a fixed order. */
+es_status es_average_lifetime(es_ctx* ctx, double* out_average);
 
 /* Waits for the context stream, then reports any device-side error flag. */
 es_status es_synchronize(es_ctx* ctx);

@@ -47,7 +47,23 @@ void es_grid_settings(const es_grid* g, es_impurity_settings* out);
  * pass to es_upload_grid so a resident copy is reused only for this grid. */
 uint64_t es_grid_generation(const es_grid* g);
 
-/* Message of the last failed es_grid_* call on this thread. */
+/* Replaces SimulationRunner::Run (src/SimulationRunner.cpp:31-50) and the
+ * executable around it (src/main.cpp): parses a reference .config file with the
+ * reference's rules (src/SimulationConfiguration.h:79-228), runs the sweep over
+ * samples, magnetic fields and temperatures on the CUDA backend, and writes the
+ * reference's results folder (<output_directory>/Result_<n>/ with the config,
+ * T<j>.dat, Metrics.txt and Sample <i>/ with sample_results.dat and the PNG
+ * maps). The folder used is copied to out_directory (out_len bytes, may be
+ * NULL). quiet != 0 suppresses the progress output. Errors, including config
+ * errors the reference exits on, return non-OK with es_host_last_error(). */
+es_status es_run_config(const char* config_path, char* out_directory, int32_t out_len, int32_t quiet);
+
+/* The parsed form of a .config file (the values es_run_config would use) as a
+ * JSON object in out_json (out_len bytes). No reference counterpart: a dry run
+ * of SimulationConfiguration::ParseFromeFile (src/SimulationConfiguration.h:79-228). */
+es_status es_config_describe(const char* config_path, char* out_json, int32_t out_len);
+
+/* Message of the last failed es_grid_* or es_run_config call on this thread. */
 const char* es_host_last_error(void);
 
 #ifdef __cplusplus
