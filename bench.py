@@ -556,9 +556,8 @@ def run_batched(args) -> None:
     torch.cuda.set_device(local)
     dev = local
     # every rank runs its own `samples` samples of the draw (weak scaling)
-    wl = workloads.config2(n_samples=max(64, args.samples * world), n_fields=args.fields)
-    wl.samples = wl.samples[rank * args.samples:(rank + 1) * args.samples]
-    wl.name = f"config2-{args.samples}x{args.fields}x3"
+    wl = workloads.shard_samples(workloads.config2(n_samples=max(64, args.samples * world), n_fields=args.fields),
+                                 rank, world, args.samples)
 
     t_tune = time.perf_counter()
     tune = autotune.tune_sweep(wl, device=dev, cache=args.tune_cache, force=args.retune)

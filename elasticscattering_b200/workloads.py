@@ -164,4 +164,20 @@ def config2(n_samples: int = 64, n_fields: int = 32, dims=(129, 257, 513), phi_s
                          impurity_radius=2e-9, target_cell_population=12, draw_seed=draw_seed)
 
 
+def shard_samples(wl: BatchWorkload, rank: int, world: int, per_rank: int) -> BatchWorkload:
+    """The samples one GPU of a multi-GPU sweep runs: rank r takes samples
+    [r * per_rank, (r + 1) * per_rank) of the draw (weak scaling: every GPU runs
+    `per_rank` samples; the passes share no data, so the only exchange is the
+    gather of the sigma results)."""
+    import copy
+    if not 0 <= rank < world or per_rank < 1:
+        raise ValueError("bad shard")
+    if (rank + 1) * per_rank > len(wl.samples):
+        raise ValueError(f"the draw holds {len(wl.samples)} samples; {world} x {per_rank} requested")
+    out = copy.copy(wl)
+    out.samples = wl.samples[rank * per_rank:(rank + 1) * per_rank]
+    out.name = f"{wl.name.split('-')[0]}-{per_rank}x{len(wl.fields)}x{len(wl.temperatures)}"
+    return out
+
+
 WORKLOADS = {"config0": config0, "config1": config1, "config3": config3}
