@@ -40,6 +40,7 @@ constexpr float kTwoPiF = 6.2831853071795864769f;
 constexpr float kPiF = 3.1415926535897932385f;
 constexpr float kGuard = 4e-6f;        // angle guard (rad): ~40x the FP32 angle error
 constexpr double kPolarGuard = 4e-6;   // |x_line - x_centre| / r below which a vertical edge is re-traced
+constexpr float kPolarMark = -2.0f;    // crossing value that marks such an edge (a miss is -1)
 
 // Where the walk reads its per-pass constants. LaunchFields: from a
 // LifetimeLaunch passed as the kernel parameter, whose fields are constant-bank
@@ -283,10 +284,9 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
     // the circle within ~kPolarGuard rad of its top or bottom, where the
     // reference's GetAngle (asin(dy / r), |dy| ~ r) can round to NaN and
     // GetNextCell then drops that crossing (cell_grid.h:80-89) -- the walk stops
-    // or takes another edge. Such lines are marked in `polar` (bit = line) and a
+    // or takes another edge. Such lines get the crossing value kPolarMark, and a
     // cell that has one hands the orbit to the FP64 re-trace.
     float la[4], lb[4];
-    unsigned polar = 0u;
     {
         const double L = f.cell_size();
         const double llx0 = f.spawn_start() + cx * L, lly0 = f.spawn_start() + cy * L;
@@ -296,7 +296,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
                                       : (e == 1 ? (llx0 + L) - o.center.x
                                                 : (e == 2 ? lly0 - o.center.y : (lly0 + L) - o.center.y));
             line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
-            if (e < 2 && fabs(c64) < kPolarGuard * r64) polar |= 1u << e;
+            if (e < 2 && fabs(c64) < kPolarGuard * r64) la[e] = kPolarMark;
         }
     }
 
@@ -306,7 +306,6 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
     int steps = 0;
 
     for (;;) {
-
         // ---- exit of this cell: first edge-line crossing after a_cur ----
         float ex = kTwoPiF, ex2 = kTwoPiF;
         int ex_line = -1, ex2_line = -1;
@@ -314,8 +313,10 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
 #pragma unroll
         for (int e = 0; e < 4; e++) {
             float a1 = la[e], a2 = lb[e];
-            if (a1 < 0.0f) continue;
-            if ((polar >> e) & 1u) ambiguous = true;  // crossing at the top or bottom of the orbit
+            if (a1 < 0.0f) {
+                if (a1 < -1.5f) ambiguous = true;  // kPolarMark: crossing at the top or bottom of the orbit
+                continue;
+            }
             if (e == entry_line) {
                 // one of the two is the entry crossing itself
                 const float d1 = fabsf(a1 - a_cur), d2 = fabsf(a2 - a_cur);
@@ -345,24 +346,6 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
         if (ex_line >= 0) {
             if (ex - a_cur < kGuard) return kSplitRetrace;                                        // tiny arc
             if (ex2_line >= 0 && ex2_line != ex_line && ex2 - ex < kGuard) return kSplitRetrace;  // corner
-            // GetNextCell's corner rule (cell_grid.h:154-167) moves diagonally when
-            // the exit point lies within 1e-7 L of a perpendicular edge. Where the
-            // orbit runs almost parallel to that edge, the point can be that close
-            // while the edge's own crossing is far away in angle, so the exit
-            // line's two crossing points are located in FP64 and checked against
-            // both perpendicular edges (2x margin).
-            const double L = f.cell_size();
-            const double llx = f.spawn_start() + cx * L, lly = f.spawn_start() + cy * L;
-            const bool horiz = ex_line >= 2;
-            const double lv = horiz ? (ex_line == 2 ? lly : lly + L) : (ex_line == 0 ? llx : llx + L);
-            const double d = lv - (horiz ? o.center.y : o.center.x);
-            const double h = sqrt(fmax(o.radius_sq - d * d, 0.0));
-            const double c_perp = horiz ? o.center.x : o.center.y;
-            const double lo = horiz ? llx : lly;
-            const double tol = 2e-7 * L;
-            const double p1 = c_perp + h, p2 = c_perp - h;
-            if (fabs(p1 - lo) < tol || fabs(p1 - (lo + L)) < tol || fabs(p2 - lo) < tol || fabs(p2 - (lo + L)) < tol)
-                return kSplitRetrace;
         }
         // Next cell across the exit line; a final visit when the orbit comes
         // full circle or the next cell leaves the grid.
@@ -379,8 +362,40 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
         const int k1 = __ldg(f.cell_end() + c);
         cnt.cells += 1;
         cnt.imps += k1 - k0;
+        // cell corner relative to the orbit centre
         const float ox = (float)((f.spawn_start() + cx * f.cell_size()) - o.center.x);
         const float oy = (float)((f.spawn_start() + cy * f.cell_size()) - o.center.y);
+        if (ex_line >= 0) {
+            // GetNextCell's corner rule (cell_grid.h:154-167) moves diagonally when
+            // the exit point lies within 1e-7 L of a perpendicular edge. Where the
+            // orbit runs almost parallel to that edge, the point can be that close
+            // while the edge's own crossing is far away in angle, so the exit
+            // line's two crossing points are checked against both perpendicular
+            // edges (2x margin): first in FP32 from the cell-local centre offset
+            // with a bound on its error (1e-5 r, valid while the exit line is not
+            // within 5% of tangency), then, only if that cannot exclude it, in FP64.
+            const float Lf = (float)f.cell_size();
+            const bool horiz = ex_line >= 2;
+            const float dl = horiz ? (ex_line == 2 ? oy : oy + Lf) : (ex_line == 0 ? ox : ox + Lf);
+            const float h32 = sqrtf(fmaxf(fmaf(-dl, dl, r * r), 0.0f));
+            const float cp = horiz ? -ox : -oy;
+            const float tol32 = 2e-7f * Lf + 1e-5f * r;
+            if (h32 < 0.05f * r || fabsf(cp + h32) < tol32 || fabsf(cp + h32 - Lf) < tol32 || fabsf(cp - h32) < tol32 ||
+                fabsf(cp - h32 - Lf) < tol32) {
+                const double L = f.cell_size();
+                const double llx = f.spawn_start() + cx * L, lly = f.spawn_start() + cy * L;
+                const double lv = horiz ? (ex_line == 2 ? lly : lly + L) : (ex_line == 0 ? llx : llx + L);
+                const double d = lv - (horiz ? o.center.y : o.center.x);
+                const double h = sqrt(fmax(o.radius_sq - d * d, 0.0));
+                const double c_perp = horiz ? o.center.x : o.center.y;
+                const double lo = horiz ? llx : lly;
+                const double tol = 2e-7 * L;
+                const double p1 = c_perp + h, p2 = c_perp - h;
+                if (fabs(p1 - lo) < tol || fabs(p1 - (lo + L)) < tol || fabs(p2 - lo) < tol ||
+                    fabs(p2 - (lo + L)) < tol)
+                    return kSplitRetrace;
+            }
+        }
         const float2* const imps32 = f.imps32();
         float v1 = 3.0e38f, v2 = 3.0e38f, v3 = 3.0e38f;  // best three crossing advances of this visit
         int k1st = -1, k2nd = -1;
@@ -436,7 +451,6 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
             entry_line = ex_line ^ 1;
             la[entry_line] = la[ex_line];
             lb[entry_line] = lb[ex_line];
-            polar = (polar & ~(1u << entry_line)) | (((polar >> ex_line) & 1u) << entry_line);
             cx = nx;
             cy = ny;
             {
@@ -447,8 +461,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
                                           : (e == 1 ? (nllx + L) - o.center.x
                                                     : (e == 2 ? nlly - o.center.y : (nlly + L) - o.center.y));
                 line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
-                polar &= ~(1u << e);
-                if (e < 2 && fabs(c64) < kPolarGuard * r64) polar |= 1u << e;
+                if (e < 2 && fabs(c64) < kPolarGuard * r64) la[e] = kPolarMark;
             }
             a_cur = ex;
             continue;
