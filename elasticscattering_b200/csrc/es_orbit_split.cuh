@@ -146,14 +146,16 @@ __device__ __forceinline__ float half_angle(float s2)
 // with an edge line at signed distance c64 (x = c for vertical lines, y = c for
 // horizontal ones); both -1 when the line misses the circle. acos(|c| / r) is
 // taken as atan2(sqrt(m (2 - m)), 1 - m) with m = (r - |c|) / r from FP64, which
-// stays accurate near tangency.
-__device__ __forceinline__ void line_crossings(double c64, double r64, float inv_r, bool horizontal, float psi0,
-                                               float dir, float& a1, float& a2)
+// stays accurate near tangency. Returns 1 when the line lies within
+// tangent_tol of tangency (| r - |c| | < tangent_tol).
+__device__ __forceinline__ unsigned line_crossings(double c64, double r64, float inv_r, bool horizontal, float psi0,
+                                                   float dir, float tangent_tol, float& a1, float& a2)
 {
     const double m64 = r64 - fabs(c64);
+    const unsigned near_tangent = fabsf((float)m64) < tangent_tol ? 1u : 0u;
     if (!(m64 > 0.0)) {
         a1 = a2 = -1.0f;
-        return;
+        return near_tangent;
     }
     const float m = (float)m64 * inv_r;
     const float ths = fast_atan2(sqrtf(m * (2.0f - m)), 1.0f - m);  // acos(|u|)
@@ -169,6 +171,7 @@ __device__ __forceinline__ void line_crossings(double c64, double r64, float inv
     }
     a1 = advance(p1, psi0, dir);
     a2 = advance(p2, psi0, dir);
+    return near_tangent;
 }
 
 // FP64 GetFirstCrossTime without the valid-range filter, as an angle: the
@@ -286,7 +289,18 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
     // GetNextCell then drops that crossing (cell_grid.h:80-89) -- the walk stops
     // or takes another edge. Such lines get the crossing value kPolarMark, and a
     // cell that has one hands the orbit to the FP64 re-trace.
+    //
+    // Bit e of `tangent` marks a line within tangent_tol of tangency
+    // (| r - |c| | < tangent_tol). GetNextCell's corner rule (cell_grid.h:154-167)
+    // moves diagonally when the exit point lies within 1e-7 L of a
+    // perpendicular edge. Where that edge's line is not near tangency, the
+    // circle crosses it within 2e-7 L / (r |cos phi|) < 2e-6 rad of the exit
+    // point (2x margin; |cos phi| > 0.1 L / r), so the exit-angle guards already
+    // hand the orbit to the FP64 re-trace; a line with |cos phi| <= 0.1 L / r
+    // at such a point has r - |c| <= r (0.1 L / r)^2 + 2e-7 L = tangent_tol.
     float la[4], lb[4];
+    unsigned tangent = 0;
+    const float tangent_tol = (float)((0.01 * f.cell_size() * f.cell_size()) * (double)inv_r + 2e-7 * f.cell_size());
     {
         const double L = f.cell_size();
         const double llx0 = f.spawn_start() + cx * L, lly0 = f.spawn_start() + cy * L;
@@ -295,7 +309,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
             const double c64 = e == 0 ? llx0 - o.center.x
                                       : (e == 1 ? (llx0 + L) - o.center.x
                                                 : (e == 2 ? lly0 - o.center.y : (lly0 + L) - o.center.y));
-            line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+            tangent |= line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, tangent_tol, la[e], lb[e]) << e;
             if (e < 2 && fabs(c64) < kPolarGuard * r64) la[e] = kPolarMark;
         }
     }
@@ -365,15 +379,14 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
         // cell corner relative to the orbit centre
         const float ox = (float)((f.spawn_start() + cx * f.cell_size()) - o.center.x);
         const float oy = (float)((f.spawn_start() + cy * f.cell_size()) - o.center.y);
-        if (ex_line >= 0) {
-            // GetNextCell's corner rule (cell_grid.h:154-167) moves diagonally when
-            // the exit point lies within 1e-7 L of a perpendicular edge. Where the
-            // orbit runs almost parallel to that edge, the point can be that close
-            // while the edge's own crossing is far away in angle, so the exit
-            // line's two crossing points are checked against both perpendicular
-            // edges (2x margin): first in FP32 from the cell-local centre offset
-            // with a bound on its error (1e-5 r, valid while the exit line is not
-            // within 5% of tangency), then, only if that cannot exclude it, in FP64.
+        if (ex_line >= 0 && (tangent & (ex_line < 2 ? 0xCu : 0x3u)) != 0) {
+            // A perpendicular edge near tangency: the orbit runs almost parallel
+            // to it, so the exit point can lie within 1e-7 L of it (the corner
+            // rule) while its own crossing is far away in angle. The exit line's
+            // two crossing points are checked against both perpendicular edges
+            // (2x margin): first in FP32 from the cell-local centre offset with a
+            // bound on its error (1e-5 r, valid while the exit line is not within
+            // 5% of tangency), then, only if that cannot exclude it, in FP64.
             const float Lf = (float)f.cell_size();
             const bool horiz = ex_line >= 2;
             const float dl = horiz ? (ex_line == 2 ? oy : oy + Lf) : (ex_line == 0 ? ox : ox + Lf);
@@ -451,6 +464,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
             entry_line = ex_line ^ 1;
             la[entry_line] = la[ex_line];
             lb[entry_line] = lb[ex_line];
+            tangent = (tangent & ~(3u << (ex_line & 2))) | (((tangent >> ex_line) & 1u) << entry_line);
             cx = nx;
             cy = ny;
             {
@@ -460,7 +474,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
                 const double c64 = e == 0 ? nllx - o.center.x
                                           : (e == 1 ? (nllx + L) - o.center.x
                                                     : (e == 2 ? nlly - o.center.y : (nlly + L) - o.center.y));
-                line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, la[e], lb[e]);
+                tangent |= line_crossings(c64, r64, inv_r, e >= 2, psi0, dir, tangent_tol, la[e], lb[e]) << e;
                 if (e < 2 && fabs(c64) < kPolarGuard * r64) la[e] = kPolarMark;
             }
             a_cur = ex;

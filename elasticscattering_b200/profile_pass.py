@@ -26,7 +26,8 @@ def main() -> None:
     ap.add_argument("--field", type=float, default=20.0)
     ap.add_argument("--coherent", type=int, default=0)
     ap.add_argument("--passes", type=int, default=1)
-    ap.add_argument("--precision", type=int, default=N.ES_PRECISION_FP64)
+    ap.add_argument("--precision", type=int, default=None,
+                    help="0 = plain FP64, 1 = FP32/FP64 split (default: FP64 per pass, split batched)")
     ap.add_argument("--variant", type=int, default=None, help="lifetime kernel variant (default: library default)")
     ap.add_argument("--time", action="store_true", help="time every variant with CUDA events")
     ap.add_argument("--compare-split", action="store_true", help="time plain FP64 against split precision")
@@ -45,7 +46,8 @@ def main() -> None:
                        w.target_cell_population)
     s = make_settings(w.tau, w.alpha, w.clockwise, w.particle_speed, w.region_size, w.region_extends, w.density,
                       w.impurity_radius, w.target_cell_population)
-    with SimulationCUDA(w.dim, w.phi_steps, g.info(), precision=a.precision) as sim:
+    prec = N.ES_PRECISION_FP64 if a.precision is None else a.precision
+    with SimulationCUDA(w.dim, w.phi_steps, g.info(), precision=prec) as sim:
         sim.InitSample(g, s, bool(a.coherent))
         if a.variant is not None:
             sim.set_tuning(lifetime_variant=a.variant)
