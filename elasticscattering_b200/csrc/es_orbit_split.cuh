@@ -47,6 +47,7 @@ constexpr float kPolarMark = -2.0f;    // crossing value that marks such an edge
 // operands and cost no registers. SharedFields: from a LifetimeLaunch in shared
 // memory (the batched kernels), loaded where the compiler chooses.
 struct LaunchFields {
+    static constexpr bool kCrossOutOfLine = true;  // see first_cross_angle
     const LifetimeLaunch& P;
     __device__ __forceinline__ const int* cell_end() const { return P.cell_end; }
     __device__ __forceinline__ const float2* imps32() const { return P.imps32; }
@@ -73,6 +74,7 @@ struct LaunchFields {
 };
 
 struct SharedFields {
+    static constexpr bool kCrossOutOfLine = false;
     const LifetimeLaunch* P;  // shared memory
     __device__ __forceinline__ const int* cell_end() const { return P->cell_end; }
     __device__ __forceinline__ const float2* imps32() const { return P->imps32; }
@@ -203,6 +205,35 @@ __device__ __forceinline__ double first_cross_angle_open(const OrbitD& o, dv2 ip
     return a_min;
 }
 
+// first_cross_angle_open as one out-of-line copy: the FP32 walk reaches it once
+// or twice per orbit (the winner) and for grazing disks. In the single-pass
+// kernel, keeping its FP64 sqrt/asin/division code out of the walk's body is
+// 3-7% faster on B200 despite the spills around the call; in the batched
+// kernel the spills cost more than the shorter body saves (measured 4-8%
+// slower), so there it stays inline (F::kCrossOutOfLine).
+__device__ __noinline__ double first_cross_angle_call(double cx, double cy, double radius, double radius_sq,
+                                                      double particle_angle, int clockwise, double ipx, double ipy,
+                                                      double ir)
+{
+    OrbitD o;
+    o.center = dv2{cx, cy};
+    o.radius = radius;
+    o.radius_sq = radius_sq;
+    o.bound_time = 0.0;
+    o.particle_angle = particle_angle;
+    o.clockwise = clockwise != 0;
+    return first_cross_angle_open(o, dv2{ipx, ipy}, ir);
+}
+
+template <class F>
+__device__ __forceinline__ double first_cross_angle(const OrbitD& o, dv2 ip, double ir)
+{
+    if (F::kCrossOutOfLine)
+        return first_cross_angle_call(o.center.x, o.center.y, o.radius, o.radius_sq, o.particle_angle,
+                                      o.clockwise ? 1 : 0, ip.x, ip.y, ir);
+    return first_cross_angle_open(o, ip, ir);
+}
+
 enum SplitOutcome : int { kSplitDone = 0, kSplitRetrace = 1 };
 
 struct SplitCounters {
@@ -214,10 +245,10 @@ template <class F>
 __device__ __forceinline__ double finish_hit(const F& f, const OrbitD& o, int win_k, int alt_k, int& flags)
 {
     const double2 q = __ldg(f.imps() + win_k);
-    double t = first_cross_angle_open(o, dv2{q.x, q.y}, f.imp_radius()) / f.w();
+    double t = first_cross_angle<F>(o, dv2{q.x, q.y}, f.imp_radius()) / f.w();
     if (alt_k >= 0) {
         const double2 a = __ldg(f.imps() + alt_k);
-        const double t2 = first_cross_angle_open(o, dv2{a.x, a.y}, f.imp_radius()) / f.w();
+        const double t2 = first_cross_angle<F>(o, dv2{a.x, a.y}, f.imp_radius()) / f.w();
         t = (t < t2) ? t : t2;
     }
     flags = kTraceOk;
@@ -424,7 +455,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
                 // grazing disk: CirclesCross and the crossing angle in FP64
                 const double2 q64 = __ldg(f.imps() + k);
                 if (!circles_cross(o, dv2{q64.x, q64.y}, f.imp_radius())) continue;
-                const double a64 = first_cross_angle_open(o, dv2{q64.x, q64.y}, f.imp_radius());
+                const double a64 = first_cross_angle<F>(o, dv2{q64.x, q64.y}, f.imp_radius());
                 if (a64 != a64) return kSplitRetrace;  // a crossing point the reference drops
                 a = (float)a64;
             } else {

@@ -34,9 +34,16 @@ def main() -> None:
     ap.add_argument("--batch", action="store_true",
                     help="run the pass through the batched kernel (one instance, fused integration)")
     ap.add_argument("--chunk-iters", type=int, default=32)
+    ap.add_argument("--sweep-sample", type=int, default=None,
+                    help="--batch: run sample K of the 64-sample batched sweep draw instead of --workload")
+    ap.add_argument("--sweep-fields", type=int, default=2, help="--sweep-sample: fields uniformly spaced 1-40 T")
+    ap.add_argument("--tcp", type=int, default=12, help="--sweep-sample: target cell population")
     a = ap.parse_args()
     if a.compare_split:
         compare_split(a)
+        return
+    if a.batch and a.sweep_sample is not None:
+        batch_sweep_sample(a)
         return
     if a.batch:
         batch_pass(a)
@@ -108,6 +115,39 @@ def batch_pass(a) -> None:
                 out, m = b.run()
     print(json.dumps({"workload": w.name, "field": a.field, "coherent": a.coherent, "orbits": w.orbits_per_pass,
                       "batch": True, "ms": ms, "metrics": m[0], "sigma": out[0, :len(w.temperatures)].tolist()}))
+
+
+def batch_sweep_sample(a) -> None:
+    """One sample of the batched sweep (its drawn start grid and density), every
+    field of --sweep-fields x both sectors x the sweep's temperatures, in one
+    batched launch."""
+    from .batch import BatchSweep, sweep_passes
+    wl = workloads.config2(n_samples=64, n_fields=a.sweep_fields)
+    smp = wl.samples[a.sweep_sample]
+    g = Grid.from_seed(smp.seed, wl.region_size, wl.region_extends, smp.density, wl.impurity_radius, a.tcp)
+    prec = N.ES_PRECISION_SPLIT if a.precision is None else a.precision
+    with BatchSweep(chunk_iters=a.chunk_iters, precision=prec) as b:
+        gid = b.add_grid(g)
+        b.set_passes(sweep_passes(wl, {smp.index: gid}, {smp.index: g.info().cell_size}, samples=[smp]))
+        ms = []
+        for _ in range(a.passes):
+            if a.time:
+                import torch
+                stream = torch.cuda.ExternalStream(b.stream_handle())
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                b.enqueue()
+                e1.record(stream)
+                out, m = b.collect()
+                ms.append(round(e0.elapsed_time(e1), 3))
+            else:
+                out, m = b.run()
+        orbits = b.total_orbits
+    print(json.dumps({"workload": wl.name, "sample": a.sweep_sample, "dim": smp.dim, "density": smp.density,
+                      "tcp": a.tcp, "fields": wl.fields, "orbits": orbits, "ms": ms,
+                      "retraced_fp64": sum(x["retraced_fp64"] for x in m),
+                      "impurities_tested": sum(x["impurities_tested"] for x in m),
+                      "cells_passed": sum(x["cells_passed"] for x in m)}))
 
 
 def compare_split(a) -> None:
