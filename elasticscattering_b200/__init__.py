@@ -8,8 +8,8 @@ include/es_cuda.h); the impurity field and the .config runner live in
 libes_host.so (include/es_host.h). This package binds both and mirrors the
 reference's Simulation/Grid interface (simulation.py).
 """
-from .simulation import (EsError, Grid, GridInformation, IterationResult, SampleMetrics, Settings, Sigma,
+from .simulation import (DeviceGrid, EsError, Grid, GridInformation, IterationResult, SampleMetrics, Settings, Sigma,
                          SimulationCUDA, make_settings)
 
-__all__ = ["EsError", "Grid", "GridInformation", "IterationResult", "SampleMetrics", "Settings", "Sigma",
+__all__ = ["DeviceGrid", "EsError", "Grid", "GridInformation", "IterationResult", "SampleMetrics", "Settings", "Sigma",
            "SimulationCUDA", "make_settings"]

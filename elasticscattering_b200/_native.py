@@ -124,6 +124,12 @@ CUDA_API = {
     "es_batch_stream": (_vp, [_vp]),
     "es_batch_launch_count": (_i64, [_vp]),
     "es_batch_total_orbits": (_i64, [_vp]),
+    "es_dgrid_create_seeded": (_i32, [_i32, _u32, _d, _d, _d, _d, _i32, _i64, C.POINTER(_vp)]),
+    "es_dgrid_destroy": (_i32, [_vp]),
+    "es_dgrid_info": (_i32, [_vp, C.POINTER(ImpuritySettings), C.POINTER(_i64), C.POINTER(_i64)]),
+    "es_dgrid_download": (_i32, [_vp, _vp, _vp]),
+    "es_upload_dgrid": (_i32, [_vp, _vp]),
+    "es_batch_add_dgrid": (_i32, [_vp, _vp, C.POINTER(_i32)]),
     "es_mlp_param_count": (_i64, []),
     "es_mlp_create": (_i32, [_i32, _i32, C.POINTER(_vp)]),
     "es_mlp_destroy": (_i32, [_vp]),

@@ -16,7 +16,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
-from .simulation import Grid, Sigma
+from .simulation import DeviceGrid, Grid, Sigma
 
 
 @dataclass
@@ -115,12 +115,16 @@ class BatchSweep:
         self._check(N.cuda_lib().es_batch_set_tuning(self._b, C.byref(t)))
         self._tuned = True
 
-    def add_grid(self, grid: Grid) -> int:
-        """Copies a host Grid to the device; returns its index for BatchPass.grid."""
+    def add_grid(self, grid) -> int:
+        """Copies a Grid (host) or DeviceGrid to the batch's device memory; returns
+        its index for BatchPass.grid."""
+        out = C.c_int32()
+        if isinstance(grid, DeviceGrid):
+            self._check(N.cuda_lib().es_batch_add_dgrid(self._b, grid.handle, C.byref(out)))
+            return int(out.value)
         xy = grid.GetImpurities()
         idx = grid.GetIndex()
         s = grid.GetSettings()
-        out = C.c_int32()
         self._check(N.cuda_lib().es_batch_add_grid(self._b, xy.ctypes.data, len(xy), idx.ctypes.data, C.byref(s),
                                                    C.byref(out)))
         return int(out.value)

@@ -42,6 +42,8 @@ CUDA_UNITS = {
     "es_lifetime_split.cu": ["-fmad=false"],
     "es_noalloc.cu": ["-fmad=false"],
     "es_batch.cu": ["-fmad=false"],
+    # grid build: the host Grid's double arithmetic, operation by operation
+    "es_grid_build.cu": ["-fmad=false"],
     # surrogate: BF16 tensor-core GEMMs and FP32 elementwise work, contraction allowed
     "es_mlp.cu": [],
 }

@@ -905,6 +905,9 @@ double fixed_point_scale(int dim, int ppq, double max_wtau)
     return std::ldexp(1.0, ex - 1);
 }
 
+es_status add_grid_arrays(es_batch* b, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
+                          const es_impurity_settings* is, cudaMemcpyKind kind, int32_t* out_grid);
+
 }  // namespace
 
 extern "C" {
@@ -1035,6 +1038,37 @@ es_status es_batch_add_grid(es_batch* b, const double* imp_xy, int64_t n_indexed
     if (prev != n_indexed)
         return bfail(b, ES_ERR_BAD_ARG, "cell index ends at %lld but %lld impurities were given", (long long)prev,
                      (long long)n_indexed);
+    return add_grid_arrays(b, imp_xy, n_indexed, cell_end, is, cudaMemcpyHostToDevice, out_grid);
+}
+
+es_status es_batch_add_dgrid(es_batch* b, const es_dgrid* grid, int32_t* out_grid)
+{
+    es_status st = bind_batch(b);
+    if (st != ES_OK) return st;
+    if (!grid || !out_grid) return bfail(b, ES_ERR_BAD_ARG, "es_batch_add_dgrid: null argument");
+    const double2* imps;
+    const int* cell_end;
+    int64_t n_indexed;
+    es_impurity_settings is;
+    uint64_t generation;
+    int device;
+    es::dgrid_arrays(grid, &imps, &cell_end, &n_indexed, &is, &generation, &device);
+    if (device != b->device)
+        return bfail(b, ES_ERR_BAD_ARG, "es_batch_add_dgrid: the grid lives on device %d, the batch on %d", device,
+                     b->device);
+    // the cell index is monotone and ends at n_indexed by construction
+    return add_grid_arrays(b, reinterpret_cast<const double*>(imps), n_indexed, cell_end, &is,
+                           cudaMemcpyDeviceToDevice, out_grid);
+}
+
+}  // extern "C"
+
+namespace {
+
+es_status add_grid_arrays(es_batch* b, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
+                          const es_impurity_settings* is, cudaMemcpyKind kind, int32_t* out_grid)
+{
+    const int64_t n_cells = (int64_t)is->cells_per_row * is->cells_per_row;
     es_batch_grid g;
     g.n_indexed = n_indexed;
     g.is = *is;
@@ -1042,10 +1076,8 @@ es_status es_batch_add_grid(es_batch* b, const double* imp_xy, int64_t n_indexed
     cudaError_t e = cudaMalloc(&g.d_imps, sizeof(double2) * n_alloc);
     if (e == cudaSuccess) e = cudaMalloc(&g.d_imps32, sizeof(float2) * n_alloc);
     if (e == cudaSuccess) e = cudaMalloc(&g.d_cell_end, sizeof(int) * n_cells);
-    if (e == cudaSuccess && n_indexed > 0)
-        e = cudaMemcpyAsync(g.d_imps, imp_xy, sizeof(double2) * n_indexed, cudaMemcpyHostToDevice, b->stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(g.d_cell_end, cell_end, sizeof(int) * n_cells, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess && n_indexed > 0) e = cudaMemcpyAsync(g.d_imps, imp_xy, sizeof(double2) * n_indexed, kind, b->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(g.d_cell_end, cell_end, sizeof(int) * n_cells, kind, b->stream);
     if (e == cudaSuccess)
         e = es::launch_local_impurities(g.d_imps, g.d_cell_end, g.d_imps32, is->spawn_region_start, is->cell_size,
                                         is->cells_per_row, b->stream);
@@ -1061,6 +1093,10 @@ es_status es_batch_add_grid(es_batch* b, const double* imp_xy, int64_t n_indexed
     *out_grid = (int32_t)(b->grids.size() - 1);
     return ES_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 es_status es_batch_clear(es_batch* b)
 {

@@ -296,6 +296,9 @@ void release(es_ctx* ctx)
     delete ctx;
 }
 
+es_status upload_arrays(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
+                        const es_impurity_settings* is, uint64_t generation, cudaMemcpyKind kind);
+
 }  // namespace
 
 extern "C" {
@@ -382,6 +385,54 @@ const char* es_last_error(const es_ctx* ctx) { return ctx ? ctx->err : g_create_
 
 void es::set_global_error(const char* msg) { snprintf(g_create_error, sizeof g_create_error, "%s", msg ? msg : ""); }
 
+namespace {
+
+es_status upload_arrays(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
+                        const es_impurity_settings* is, uint64_t generation, cudaMemcpyKind kind)
+{
+    const int64_t n_cells = (int64_t)is->cells_per_row * is->cells_per_row;
+    if (n_indexed > ctx->imps_cap) {
+        cudaFree(ctx->d_imps);
+        ctx->d_imps = nullptr;
+        ctx->imps_cap = 0;
+        ES_CUDA(cudaMalloc(&ctx->d_imps, sizeof(double2) * (n_indexed > 0 ? n_indexed : 1)), "impurity buffer");
+        ctx->imps_cap = n_indexed;
+    }
+    if (n_cells > ctx->cells_cap) {
+        cudaFree(ctx->d_cell_end);
+        ctx->d_cell_end = nullptr;
+        ctx->cells_cap = 0;
+        ES_CUDA(cudaMalloc(&ctx->d_cell_end, sizeof(int) * n_cells), "cell index buffer");
+        ctx->cells_cap = n_cells;
+    }
+    if (n_indexed > 0)
+        ES_CUDA(cudaMemcpyAsync(ctx->d_imps, imp_xy, sizeof(double2) * n_indexed, kind, ctx->stream),
+                "impurity upload");
+    ES_CUDA(cudaMemcpyAsync(ctx->d_cell_end, cell_end, sizeof(int) * n_cells, kind, ctx->stream), "cell index upload");
+    if (ctx->desc.precision == ES_PRECISION_SPLIT) {
+        if (n_indexed > ctx->imps32_cap) {
+            cudaFree(ctx->d_imps32);
+            ctx->d_imps32 = nullptr;
+            ctx->imps32_cap = 0;
+            ES_CUDA(cudaMalloc(&ctx->d_imps32, sizeof(float2) * (n_indexed > 0 ? n_indexed : 1)), "FP32 impurity buffer");
+            ctx->imps32_cap = n_indexed;
+        }
+        ES_CUDA(es::launch_local_impurities(ctx->d_imps, ctx->d_cell_end, ctx->d_imps32, is->spawn_region_start,
+                                            is->cell_size, is->cells_per_row, ctx->stream),
+                "FP32 impurity conversion");
+        ctx->launches++;
+    }
+    ES_CUDA(cudaStreamSynchronize(ctx->stream), "grid upload");
+    ctx->n_imps = n_indexed;
+    ctx->is = *is;
+    ctx->generation = generation;
+    ctx->has_grid = true;
+    ctx->lifetimes_valid = false;
+    return ES_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 es_status es_get_tuning(const es_ctx* ctx, es_tuning* out)
@@ -422,46 +473,28 @@ es_status es_upload_grid(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, c
     if (prev != n_indexed)
         return fail(ctx, ES_ERR_BAD_ARG, "cell index ends at %lld but %lld impurities were given", (long long)prev,
                     (long long)n_indexed);
+    return upload_arrays(ctx, imp_xy, n_indexed, cell_end, is, generation, cudaMemcpyHostToDevice);
+}
 
-    if (n_indexed > ctx->imps_cap) {
-        cudaFree(ctx->d_imps);
-        ctx->d_imps = nullptr;
-        ctx->imps_cap = 0;
-        ES_CUDA(cudaMalloc(&ctx->d_imps, sizeof(double2) * (n_indexed > 0 ? n_indexed : 1)), "impurity buffer");
-        ctx->imps_cap = n_indexed;
-    }
-    if (n_cells > ctx->cells_cap) {
-        cudaFree(ctx->d_cell_end);
-        ctx->d_cell_end = nullptr;
-        ctx->cells_cap = 0;
-        ES_CUDA(cudaMalloc(&ctx->d_cell_end, sizeof(int) * n_cells), "cell index buffer");
-        ctx->cells_cap = n_cells;
-    }
-    if (n_indexed > 0)
-        ES_CUDA(cudaMemcpyAsync(ctx->d_imps, imp_xy, sizeof(double2) * n_indexed, cudaMemcpyHostToDevice, ctx->stream),
-                "impurity upload");
-    ES_CUDA(cudaMemcpyAsync(ctx->d_cell_end, cell_end, sizeof(int) * n_cells, cudaMemcpyHostToDevice, ctx->stream),
-            "cell index upload");
-    if (ctx->desc.precision == ES_PRECISION_SPLIT) {
-        if (n_indexed > ctx->imps32_cap) {
-            cudaFree(ctx->d_imps32);
-            ctx->d_imps32 = nullptr;
-            ctx->imps32_cap = 0;
-            ES_CUDA(cudaMalloc(&ctx->d_imps32, sizeof(float2) * (n_indexed > 0 ? n_indexed : 1)), "FP32 impurity buffer");
-            ctx->imps32_cap = n_indexed;
-        }
-        ES_CUDA(es::launch_local_impurities(ctx->d_imps, ctx->d_cell_end, ctx->d_imps32, is->spawn_region_start,
-                                            is->cell_size, is->cells_per_row, ctx->stream),
-                "FP32 impurity conversion");
-        ctx->launches++;
-    }
-    ES_CUDA(cudaStreamSynchronize(ctx->stream), "grid upload");
-    ctx->n_imps = n_indexed;
-    ctx->is = *is;
-    ctx->generation = generation;
-    ctx->has_grid = true;
-    ctx->lifetimes_valid = false;
-    return ES_OK;
+es_status es_upload_dgrid(es_ctx* ctx, const es_dgrid* g)
+{
+    es_status st = bind(ctx);
+    if (st != ES_OK) return st;
+    if (!g) return fail(ctx, ES_ERR_BAD_ARG, "es_upload_dgrid: null grid");
+    const double2* imps;
+    const int* cell_end;
+    int64_t n_indexed;
+    es_impurity_settings is;
+    uint64_t generation;
+    int device;
+    es::dgrid_arrays(g, &imps, &cell_end, &n_indexed, &is, &generation, &device);
+    if (device != ctx->device)
+        return fail(ctx, ES_ERR_BAD_ARG, "es_upload_dgrid: the grid lives on device %d, the context on %d", device,
+                    ctx->device);
+    if (ctx->has_grid && generation == ctx->generation) return ES_OK;
+    // the cell index is monotone and ends at n_indexed by construction
+    return upload_arrays(ctx, reinterpret_cast<const double*>(imps), n_indexed, cell_end, &is, generation,
+                         cudaMemcpyDeviceToDevice);
 }
 
 es_status es_init_sample(es_ctx* ctx, const es_settings* s, int32_t coherent)

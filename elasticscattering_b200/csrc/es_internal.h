@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include "es_cuda.h"
+
 #include <cstdint>
 
 namespace es {
@@ -101,6 +103,10 @@ struct IntegrateLaunch {
 
 // Message returned by es_last_error(NULL), for entry points without a context.
 void set_global_error(const char* msg);
+
+// The device arrays of a grid built by es_dgrid_create_seeded (es_grid_build.cu).
+void dgrid_arrays(const es_dgrid* g, const double2** imps, const int** cell_end, int64_t* n_indexed,
+                  es_impurity_settings* is, uint64_t* generation, int* device);
 
 cudaError_t launch_lifetimes_fp64(const LifetimeLaunch& L, cudaStream_t s);
 // Split precision: FP32 walk, then the FP64 re-trace of the listed orbits (two launches).

@@ -139,6 +139,79 @@ class Grid:
                                self.GetTotalImpurityCount(), self.GetCellsPerRow() ** 2)
 
 
+class DeviceGrid:
+    """The seeded Grid built on the GPU (es_dgrid_create_seeded): the host Grid's
+    impurity positions, ordered array and cell index, bit for bit, without the
+    host build or the upload. Same getters as Grid (copies to the host)."""
+
+    def __init__(self, handle: int, region_size: float, region_extends: float, seed: int, device: int):
+        self._h = C.c_void_p(handle)
+        self.region_size = region_size
+        self.region_extends = region_extends
+        self.seed = seed
+        self.device = device
+
+    @classmethod
+    def from_seed(cls, seed: int, region_size: float, region_extends: float, density: float,
+                  impurity_radius: float, target_cell_population: int, max_impurities: int = 0,
+                  device: int = 0) -> "DeviceGrid":
+        h = C.c_void_p()
+        N.check(N.cuda_lib().es_dgrid_create_seeded(int(device), seed & 0xFFFFFFFF, region_size, region_extends,
+                                                    density, impurity_radius, int(target_cell_population),
+                                                    int(max_impurities), C.byref(h)), None)
+        return cls(h.value, region_size, region_extends, seed, device)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            N.cuda_lib().es_dgrid_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def _info(self):
+        s = ImpuritySettings()
+        n_idx, n_unique = C.c_int64(), C.c_int64()
+        N.check(N.cuda_lib().es_dgrid_info(self._h, C.byref(s), C.byref(n_idx), C.byref(n_unique)), None)
+        return s, int(n_idx.value), int(n_unique.value)
+
+    def GetTotalImpurityCount(self) -> int:
+        return self._info()[1]
+
+    def GetUniqueImpurityCount(self) -> int:
+        return self._info()[2]
+
+    def GetCellsPerRow(self) -> int:
+        return int(self._info()[0].cells_per_row)
+
+    def GetSeed(self) -> int:
+        return self.seed
+
+    def GetSettings(self) -> ImpuritySettings:
+        return self._info()[0]
+
+    def GetImpurities(self) -> np.ndarray:
+        n = self.GetTotalImpurityCount()
+        out = np.zeros((n, 2))
+        if n:
+            N.check(N.cuda_lib().es_dgrid_download(self._h, out.ctypes.data, None), None)
+        return out
+
+    def GetIndex(self) -> np.ndarray:
+        c = self.GetCellsPerRow()
+        out = np.zeros(c * c, dtype=np.int32)
+        N.check(N.cuda_lib().es_dgrid_download(self._h, None, out.ctypes.data), None)
+        return out
+
+    def info(self) -> "GridInformation":
+        s, n_idx, _ = self._info()
+        return GridInformation(self.region_size, self.region_extends, s.cell_size, n_idx, s.cells_per_row ** 2)
+
+
 @dataclass
 class GridInformation:
     """GridInformation, reference src/sim/es/settings.h:65-73."""
@@ -186,7 +259,10 @@ class SimulationCUDA:
     def _check(self, st: int) -> None:
         N.check(st, self._ctx)
 
-    def _upload(self, grid: Grid) -> None:
+    def _upload(self, grid) -> None:
+        if isinstance(grid, DeviceGrid):
+            self._check(N.cuda_lib().es_upload_dgrid(self._ctx, grid.handle))
+            return
         xy = grid.GetImpurities()
         idx = grid.GetIndex()
         s = grid.GetSettings()

@@ -326,6 +326,36 @@ int64_t es_batch_launch_count(const es_batch* b);
 int64_t es_batch_total_orbits(const es_batch* b);
 
 /* ---------------------------------------------------------------------------
+ * Grids built on the GPU. Replaces the host work of Grid::Grid(seed, ...)
+ * (src/sim/Grid.cpp:28-46) with GenerateImpurities, GenerateImpurityCells and
+ * ConvertToIndex (src/sim/Grid.cpp:61-110, :112-188) plus the upload of
+ * es_upload_grid / es_batch_add_grid: the impurity positions are the
+ * libstdc++ minstd_rand0 + generate_canonical draws the host Grid makes,
+ * reproduced draw for draw, and the ordered array and cumulative cell index
+ * are the host Grid's bit for bit. Failures before a grid exists report
+ * through es_last_error(NULL).
+ * ------------------------------------------------------------------------- */
+
+typedef struct es_dgrid es_dgrid;
+
+/* Grid(seed, region_size, region_extends, density, impurity_radius,
+ * target_cell_population) on device_ordinal. max_impurities <= 0 means the
+ * reference's 1e7 ("Woah!", src/sim/Grid.cpp:36). */
+es_status es_dgrid_create_seeded(int32_t device_ordinal, uint32_t seed, double region_size, double region_extends,
+                                 double density, double impurity_radius, int32_t target_cell_population,
+                                 int64_t max_impurities, es_dgrid** out);
+es_status es_dgrid_destroy(es_dgrid* g);
+/* GetSettings (src/sim/Grid.h:77-86), GetTotalImpurityCount and the unique count. */
+es_status es_dgrid_info(const es_dgrid* g, es_impurity_settings* out_settings, int64_t* out_indexed,
+                        int64_t* out_unique);
+/* GetImpurities / GetIndex as host copies: 2 * n_indexed doubles, cells_per_row^2 ints (either may be NULL). */
+es_status es_dgrid_download(const es_dgrid* g, double* out_xy, int32_t* out_cell_end);
+/* es_upload_grid from a device grid (device-to-device; skipped when already resident). */
+es_status es_upload_dgrid(es_ctx* ctx, const es_dgrid* g);
+/* es_batch_add_grid from a device grid (device-to-device copy; g may be destroyed afterwards). */
+es_status es_batch_add_dgrid(es_batch* b, const es_dgrid* g, int32_t* out_grid);
+
+/* ---------------------------------------------------------------------------
  * Learned surrogate. No reference counterpart: an ensemble of MLPs,
  * 5 -> 256 x 4 -> 2 with GELU; the hidden layers in BF16 weights and
  * activations with FP32 accumulation on the tensor cores, the 256 -> 2 head in
