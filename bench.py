@@ -715,6 +715,25 @@ def run_batched(args) -> None:
     h2d = sum(g.GetTotalImpurityCount() * 16 + g.GetCellsPerRow() ** 2 * 4 for g in grids)
     d2h = n_pass * (N.ES_BATCH_MAX_T * 2 * 8 + 10 * 8)
 
+    # end to end from the sweep's seeds: every sample's grid built on the GPU
+    # (bit-identical to the host Grid), then the same run and readback
+    from elasticscattering_b200 import DeviceGrid
+    torch.cuda.synchronize()
+    t_seed = time.perf_counter()
+    bd = BatchSweep(dev, precision=N.ES_PRECISION_SPLIT, **tune.shape)
+    did = {}
+    for s in wl.samples:
+        dg = DeviceGrid.from_seed(s.seed, wl.region_size, wl.region_extends, s.density, wl.impurity_radius,
+                                  tcp_for(s.density), device=dev)
+        did[s.index] = bd.add_grid(dg)
+        dg.close()
+    device_grid_s = time.perf_counter() - t_seed
+    bd.set_passes(sweep_passes(wl, did, cell))
+    out_seed, _ = bd.run(with_metrics=True)
+    seed_s = time.perf_counter() - t_seed
+    bd.close()
+    seeds_match = bool(np.array_equal(out_seed, out_split))
+
     peak32 = C.c_double(0.0)
     N.check(N.cuda_lib().es_probe_fp32_fma(dev, C.byref(peak32)))
     if world > 1:
@@ -753,8 +772,13 @@ def run_batched(args) -> None:
                             "points_per_sec": plain_pps, "split_batch_same_work_points_per_sec": sub_pps,
                             "speedup_same_work": sub_pps / plain_pps, "max_rel_vs_plain_fp64": worst_vs_plain},
         "host_grid_build_s": grid_build_s,
+        "device_grid_build_s": device_grid_s,
         "e2e": {"value": orbits / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "seconds": e2e_s, "note": "BatchSweep with host grids: copies, graph record, run, readback"},
+        "e2e_from_seeds": {"value": orbits / seed_s, "unit": UNIT, "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": d2h, "seconds": seed_s, "sigma_equal_to_host_grid_run": seeds_match,
+                           "note": "grids built on the GPU from the sweep's seeds inside the timed region "
+                                   "(DeviceGrid), graph record, run, readback"},
     }
     if cpu:
         line["cpu_baseline"] = {"value": cpu["rate"], "unit": UNIT, "cores": cpu["procs"], "kind": "reference",
@@ -850,10 +874,34 @@ def run_surrogate(args) -> None:
         "training": {"grid_build_s": build_s, "data_s": data_s, "train_s": train_s_time,
                      "final_loss": losses[-1]},
         "gpu_launches": ens.launch_count(),
+        # the queries arrive as host arrays and the answers return to the host on every call
+        "e2e": {"value": calibrated["queries_per_sec"], "unit": "queries/s", "h2d_bytes_per_step": Q * 5 * 4,
+                "d2h_bytes_per_step": Q * (ens.n_nets * 2 + 2 + 2) * 4,
+                "note": "Surrogate.query on host arrays: features in, member/mean/spread out, simulator fallback"},
+        "roofline": mlp_roofline(Q, ens.n_nets, statistics.median([calibrated["network_ms_per_batch"],
+                                                                    stated["network_ms_per_batch"]])),
     }
     ens.close()
     sim.close()
     print(json.dumps(line))
+
+
+def mlp_roofline(q: int, n_nets: int, ms: float) -> dict:
+    """The network pass of one serving batch against the measured dense BF16 rate:
+    2 flops per multiply-add of the 5-256-256-256-256-2 layers, every member."""
+    macs = 5 * 256 + 3 * 256 * 256 + 256 * 2
+    flops = 2.0 * q * n_nets * macs
+    peak, src = None, "MEASURED_PEAKS.json absent: fallback 1590 TFLOP/s"
+    try:
+        peak = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops"])
+        src = "MEASURED_PEAKS.json bf16_tflops (burst, cuBLAS bf16 GEMM)"
+    except Exception:
+        peak = 1590.0
+    achieved = flops / (ms * 1e-3) / 1e12
+    return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "gemm_kernel (BF16 mma.sync, FP32 accumulate) + head_forward_kernel",
+            "work": f"{flops:.3g} flops per {q}-query batch, {n_nets} members", "peak_source": src,
+            "note": "latency-bound: a 4096 x 256 x 256 layer is 0.27 GFLOP, a few microseconds at peak"}
 
 
 def profiled_traffic(name: str):

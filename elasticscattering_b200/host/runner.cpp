@@ -17,7 +17,6 @@
 #include <iostream>
 #include <memory>
 #include <sstream>
-#include <thread>
 
 #include "es_host.h"
 #include "logger.h"
@@ -133,28 +132,6 @@ SimulationResult SimulationRunner::RunBatched()
 {
     const int S = cfg_.num_samples, N = (int)cfg_.magnetic_fields.size(), T = (int)cfg_.temperatures.size();
     if (T > ES_BATCH_MAX_T) throw SimulationError("batched runs take at most 8 temperatures");
-    // every sample's grid, built on host threads
-    std::vector<std::unique_ptr<Grid>> grids((size_t)S);
-    const double tg = now_s();
-    {
-        std::vector<std::thread> pool;
-        const int threads = std::max(1, std::min(S, (int)std::thread::hardware_concurrency()));
-        for (int w = 0; w < threads; w++)
-            pool.emplace_back([&, w]() {
-                for (int s = w; s < S; s += threads) grids[(size_t)s] = std::make_unique<Grid>(make_grid(cfg_, s));
-            });
-        for (auto& t : pool) t.join();
-    }
-    const double grid_time = (now_s() - tg) / S;
-    if (cfg_.output_type != OutputType::Nothing) {
-        GlobalMetrics gm;
-        gm.particles_per_row = cfg_.positions_per_row;
-        gm.phi_steps = 4 * cfg_.particles_per_quadrant;
-        gm.cells_per_row = grids[0]->GetCellsPerRow();
-        gm.unique_impurity_count = grids[0]->GetUniqueImpurityCount();
-        gm.grid_creation_time = grid_time;
-        Logger::CreateSampleMetricsLog(MetricsPath(), gm);
-    }
     es_batch* b = nullptr;
     if (es_batch_create(cfg_.device_ordinal, &b) != ES_OK) throw SimulationError(es_last_error(nullptr));
     std::unique_ptr<es_batch, es_status (*)(es_batch*)> guard(b, es_batch_destroy);
@@ -165,16 +142,43 @@ SimulationResult SimulationRunner::RunBatched()
     check(es_batch_get_tuning(b, &tu));
     tu.precision = cfg_.precision;
     check(es_batch_set_tuning(b, &tu));
+
+    // Every sample's Grid (src/SimulationRunner.cpp:60,96-97) built on the GPU
+    // (es_dgrid: the host Grid's arrays bit for bit) and copied into the batch.
+    struct SampleGrid {
+        es_impurity_settings is{};
+        int64_t indexed = 0, unique = 0;
+        uint32_t seed = 0;
+    };
+    std::vector<SampleGrid> grids((size_t)S);
     std::vector<int32_t> ids((size_t)S);
+    const double tg = now_s();
     for (int s = 0; s < S; s++) {
-        const Grid& g = *grids[(size_t)s];
-        const es_impurity_settings is = g.GetSettings();
-        check(es_batch_add_grid(b, &g.GetImpurities()[0].x, g.GetTotalImpurityCount(), g.GetIndex().data(), &is,
-                                &ids[(size_t)s]));
+        const es_settings& st = cfg_.settings;
+        es_dgrid* dg = nullptr;
+        if (es_dgrid_create_seeded(cfg_.device_ordinal, cfg_.sample_seeds[(size_t)s], st.region_size,
+                                   st.region_extends, st.impurity_density, st.impurity_radius,
+                                   st.target_cell_population, 0, &dg) != ES_OK)
+            throw SimulationError(es_last_error(nullptr));
+        std::unique_ptr<es_dgrid, es_status (*)(es_dgrid*)> dguard(dg, es_dgrid_destroy);
+        SampleGrid& g = grids[(size_t)s];
+        if (es_dgrid_info(dg, &g.is, &g.indexed, &g.unique) != ES_OK) throw SimulationError(es_last_error(nullptr));
+        g.seed = cfg_.sample_seeds[(size_t)s];
+        check(es_batch_add_dgrid(b, dg, &ids[(size_t)s]));
+    }
+    const double grid_time = (now_s() - tg) / S;
+    if (cfg_.output_type != OutputType::Nothing) {
+        GlobalMetrics gm;
+        gm.particles_per_row = cfg_.positions_per_row;
+        gm.phi_steps = 4 * cfg_.particles_per_quadrant;
+        gm.cells_per_row = grids[0].is.cells_per_row;
+        gm.unique_impurity_count = grids[0].unique;
+        gm.grid_creation_time = grid_time;
+        Logger::CreateSampleMetricsLog(MetricsPath(), gm);
     }
     // The reference takes GridInformation::cell_size from the first sample's grid
     // for every sample (src/SimulationRunner.cpp:76-86).
-    const double cell0 = grids[0]->GetSettings().cell_size;
+    const double cell0 = grids[0].is.cell_size;
     std::vector<es_batch_instance> inst;
     for (int s = 0; s < S; s++)
         for (int coh = 1; coh >= 0; coh--)
@@ -207,11 +211,11 @@ SimulationResult SimulationRunner::RunBatched()
         for (int coh = 1; coh >= 0; coh--) {
             SampleResult res(T, N);
             SampleMetrics sm(s, coh == 1, nlt);
-            const Grid& g = *grids[(size_t)s];
-            sm.total_indexed_impurities = g.GetTotalImpurityCount();
-            sm.impurity_count = g.GetUniqueImpurityCount();
-            sm.total_cells = (int64_t)g.GetCellsPerRow() * g.GetCellsPerRow();
-            sm.seed = g.GetSeed();
+            const SampleGrid& g = grids[(size_t)s];
+            sm.total_indexed_impurities = g.indexed;
+            sm.impurity_count = g.unique;
+            sm.total_cells = (int64_t)g.is.cells_per_row * g.is.cells_per_row;
+            sm.seed = g.seed;
             for (int i = 0; i < N; i++, k++) {
                 for (int t = 0; t < T; t++)
                     res.results[(size_t)i][(size_t)t] = Sigma(out[(k * ES_BATCH_MAX_T + t) * 2],
