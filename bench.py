@@ -809,6 +809,9 @@ def run_surrogate(args) -> None:
     ens = S.MLPEnsemble(4, dev)
     sur = S.Surrogate(ens, sim, tolerance=0.01)
     t0 = time.perf_counter()
+    # Adam at 2e-3, halved after each quarter of the run. (48k steps with 8 halvings fit the
+    # validation set slightly better, p95 1.29 % against 1.40 %, but the members then agree so
+    # closely that their spread stops flagging the queries the network gets wrong.)
     losses = sur.fit(train_q, train_s, steps=args.train_steps, batch=256, lr=2e-3, seed=0)
     train_s_time = time.perf_counter() - t0
     # fallback threshold: calibrated on held-out simulator answers so that the

@@ -31,6 +31,7 @@
 #include "es_cuda.h"
 #include "es_host_math.h"
 #include "es_orbit_split.cuh"
+#include "es_sigma32.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -97,64 +98,11 @@ __device__ __forceinline__ double simpson_w(int i, int dim)
     return (i == 0 || i == dim - 1) ? 1.0 : main_multiplier;
 }
 
-// sin and cos of an FP64 angle, evaluated in FP32. The quadrant reduction
-// x = q pi/2 + r, |r| <= pi/4, is done in FP64 (exact enough for any |x| the
-// kernel meets, a few thousand radians at most); sin r and cos r are their
-// Taylor polynomials (degree 9 and 10: truncation below 2e-9 on |r| <= pi/4),
-// evaluated by Horner's rule in FP32. Measured against FP64 sin/cos over
-// [-50, 50] and down to |x| = 1e-12: at most 1.5 ulp. The code is short and
-// branch-free, which matters in a kernel limited by instruction fetch.
-__device__ __forceinline__ void sincos_reduced(double x, float& s_out, float& c_out)
-{
-    constexpr double kTwoOverPi = 0.636619772367581343076;
-    constexpr double kHalfPi = 1.570796326794896619231;
-    const double q = rint(x * kTwoOverPi);
-    const float r = (float)(x - q * kHalfPi);
-    const float r2 = r * r;
-    const float s = r + r * r2 * (-1.0f / 6.0f + r2 * (1.0f / 120.0f + r2 * (-1.0f / 5040.0f + r2 * (1.0f / 362880.0f))));
-    const float c = 1.0f + r2 * (-0.5f + r2 * (1.0f / 24.0f + r2 * (-1.0f / 720.0f + r2 * (1.0f / 40320.0f +
-                                                                                             r2 * (-1.0f / 3628800.0f)))));
-    const int n = ((int)(long long)q) & 3;
-    s_out = (n == 0) ? s : (n == 1) ? c : (n == 2) ? -s : -c;
-    c_out = (n == 0) ? c : (n == 1) ? -s : (n == 2) ? -c : s;
-}
-
-// 1 - exp(-x) for x >= 0 in FP32: the Taylor series (degree 8, nested) below
-// 0.5, where 1 - exp(-x) would cancel; 1 - expf(-x) above. Relative error
-// below 2e-7 on [1e-10, 15].
-__device__ __forceinline__ float one_minus_exp_neg(float x)
-{
-    if (x < 0.5f)
-        return x * (1.0f - x * 0.5f * (1.0f - x * (1.0f / 3.0f) * (1.0f - x * 0.25f * (1.0f - x * 0.2f *
-               (1.0f - x * (1.0f / 6.0f) * (1.0f - x * (1.0f / 7.0f) * (1.0f - x * 0.125f)))))));
-    return 1.0f - expf(-x);
-}
-
-// GetSigma (src/sim/es/util.h:34-46) for the truncated lifetimes of one orbit,
-// FP32. With z = exp(-t/tau), e1 = 1 - z, h = w t / 2:
-//   cos(phi) - z cos(phi + 2h)       = cos(phi) e1 + 2 z sin(h) sin(phi + h)
-//   w tau (z sin(phi + 2h) - sin(phi)) = w tau (2 z sin(h) cos(phi + h) - e1 sin(phi))
-// Both right-hand sides are sums of products of well-conditioned factors, so
-// each orbit's value keeps FP32 relative accuracy even for t << tau, where
-// the left-hand sides cancel (there FP32 loses up to 1e-5 of sigma_xy). The
-// angles h and phi + h are formed and reduced in FP64.
+// GetSigma of pass I's temperature k for one orbit (sigma_fp32).
 __device__ __forceinline__ void kernel_fp32(const BatchInstanceD& I, int k, double raw, const PhaseSigma& ph,
                                             float& r_xx, float& r_xy)
 {
-    const float c = (float)ph.cos_phi, s = (float)ph.sin_phi;
-    const double max_lt = I.max_lt[k];
-    const double lt = raw < max_lt ? raw : max_lt;
-    const float e1 = one_minus_exp_neg((float)(lt * I.inv_tau[k]));
-    const float z = 1.0f - e1;
-    const double h = 0.5 * I.w_signed * lt;
-    float sh, ch, sp, cp;
-    sincos_reduced(h, sh, ch);
-    sincos_reduced(ph.phi + h, sp, cp);
-    const float zs = 2.0f * z * sh;
-    const float wt = (float)I.wtau[k];
-    const float r = c * e1 + zs * sp + wt * (zs * cp - e1 * s);
-    r_xx = r * c;
-    r_xy = r * s;
+    sigma_fp32(raw, I.max_lt[k], I.inv_tau[k], I.w_signed, I.wtau[k], ph, r_xx, r_xy);
 }
 
 __device__ __forceinline__ void add_kernel_fp32(const BatchInstanceD& I, double raw, const PhaseSigma& ph,

@@ -202,6 +202,7 @@ es_status enqueue_integrate(es_ctx* ctx, const double* temperatures, int32_t n_t
             const double tau = get_tau(ctx, T);
             L.tau[k] = tau;
             L.max_lt[k] = 15.0 * tau;  // GetDefaultMaxLifetime, Simulation.h:91
+            L.inv_tau[k] = 1.0 / tau;
             L.factor[k] = integrand_factor(ctx, w, tau);
         }
         if (pos) {
@@ -217,6 +218,7 @@ es_status enqueue_integrate(es_ctx* ctx, const double* temperatures, int32_t n_t
         L.n_phase = ctx->n_phase;
         L.n_t = nc;
         L.n_blocks = es::kIntegrateBlocks;
+        L.fp32 = ctx->desc.precision == ES_PRECISION_SPLIT ? 1 : 0;
         ES_CUDA(es::launch_integrate(L, ctx->stream), "integration kernel launch");
         ctx->launches += 2;
     }

@@ -17,7 +17,13 @@
 // partial per temperature; a second single-block kernel sums the partials in a
 // fixed order and applies GetSigmaIntegrandFactor. Every summation order is
 // fixed, so results are bit-reproducible run to run.
+//
+// Split-precision contexts (fp32 = 1) evaluate GetSigma in FP32 (es_sigma32.cuh:
+// cancellation-free form, angles formed and reduced in FP64) and keep every
+// sum in FP64, as the north-star split asks of the Simpson integrals; the
+// plain path keeps the reference's FP64 expression operation by operation.
 #include "es_internal.h"
+#include "es_sigma32.cuh"
 
 namespace es {
 
@@ -38,10 +44,13 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-template <int NT>
-__global__ void __launch_bounds__(kIntegrateThreads) integrate_positions_kernel(IntegrateLaunch P)
+// kThreads: 512 for one or two temperatures (two blocks of 16 warps per SM at
+// <= 64 registers: the lifetime loads of 32 warps in flight per SM), 256 above
+// (more accumulators per thread).
+template <int NT, bool kFP32, int kThreads>
+__global__ void __launch_bounds__(kThreads, 2) integrate_positions_kernel(IntegrateLaunch P)
 {
-    constexpr int kWarps = kIntegrateThreads / 32;
+    constexpr int kWarps = kThreads / 32;
     __shared__ double s_acc[kWarps][NT][2];
 
     const int lane = threadIdx.x & 31;
@@ -69,6 +78,21 @@ __global__ void __launch_bounds__(kIntegrateThreads) integrate_positions_kernel(
         for (int v = lane; v < P.n_phase; v += 32) {
             const double raw = __ldg(lts + v);
             const PhaseSigma ph = P.phase[v];
+            if (kFP32) {
+                const SigmaAngles a_raw = sigma_angles(raw, P.w_signed, ph);
+#pragma unroll
+                for (int k = 0; k < NT; k++) {
+                    const bool keep = raw < max_lt[k];
+                    const double lt = keep ? raw : max_lt[k];
+                    const SigmaAngles a = keep ? a_raw : sigma_angles(lt, P.w_signed, ph);
+                    float r_xx, r_xy;
+                    sigma_fp32_at(a, lt, P.inv_tau[k], wtau[k], ph, r_xx, r_xy);
+                    acc_xx[k] += (double)r_xx * ph.weight;
+                    acc_xy[k] += (double)r_xy * ph.weight;
+                    acc_lt[k] += lt * ph.weight;
+                }
+                continue;
+            }
             double sa_raw, ca_raw;
             sincos(ph.phi + P.w_signed * raw, &sa_raw, &ca_raw);
 #pragma unroll
@@ -181,7 +205,9 @@ __global__ void __launch_bounds__(256) sum_partials_kernel(const double* partial
 template <int NT>
 cudaError_t launch_group(const IntegrateLaunch& L, cudaStream_t s)
 {
-    integrate_positions_kernel<NT><<<L.n_blocks, kIntegrateThreads, 0, s>>>(L);
+    constexpr int kThreads = NT <= 2 ? 2 * kIntegrateThreads : kIntegrateThreads;
+    if (L.fp32) integrate_positions_kernel<NT, true, kThreads><<<L.n_blocks, kThreads, 0, s>>>(L);
+    else integrate_positions_kernel<NT, false, kThreads><<<L.n_blocks, kThreads, 0, s>>>(L);
     return cudaGetLastError();
 }
 

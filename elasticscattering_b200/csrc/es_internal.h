@@ -79,7 +79,7 @@ enum LifetimeVariant : int {
 };
 
 constexpr int kIntegrateBlocks = 296;   // 2 x 148 SMs; fixed so the reduction order is fixed
-constexpr int kIntegrateThreads = 256;
+constexpr int kIntegrateThreads = 256;   // threads per block for 3+ temperatures; 1-2 temperatures use 512
 constexpr int kMaxTChunk = 8;           // temperatures integrated per pass over the lifetimes
 
 // One group of up to kMaxTChunk temperatures; all per-temperature constants
@@ -89,6 +89,7 @@ struct IntegrateLaunch {
     const PhaseSigma* phase;
     double tau[kMaxTChunk];       // GetTau per temperature
     double max_lt[kMaxTChunk];    // GetDefaultMaxLifetime = 15 * tau
+    double inv_tau[kMaxTChunk];   // 1 / tau (the FP32 kernel)
     double factor[kMaxTChunk];    // GetSigmaIntegrandFactor
     double* pos_lt;               // optional per-position maps [t][pos] (images), may be null
     double* pos_xx;
@@ -99,6 +100,7 @@ struct IntegrateLaunch {
     double phi_integrand_factor;
     int dim, n_phase, n_t;        // n_t <= kMaxTChunk
     int n_blocks;                 // partial blocks per temperature
+    int fp32;                     // 1: the FP32 Boltzmann kernel of the split path (es_sigma32.cuh)
 };
 
 // Message returned by es_last_error(NULL), for entry points without a context.

@@ -98,7 +98,10 @@ class Grid:
 
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value:
-            N.host_lib().es_grid_destroy(self._h)
+            try:
+                N.host_lib().es_grid_destroy(self._h)
+            except Exception:  # interpreter shutdown: the library may already be gone
+                pass
             self._h = C.c_void_p()
 
     @property
@@ -167,7 +170,10 @@ class DeviceGrid:
             self._h = C.c_void_p()
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may already be gone
+            pass
 
     @property
     def handle(self) -> C.c_void_p:

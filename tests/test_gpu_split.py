@@ -136,3 +136,30 @@ def test_split_reproduces_reference_rounding_cases(cuda_device, sample, coherent
     finally:
         plain.close()
         split.close()
+
+
+def test_split_images_and_fp32_integration(cuda_device):
+    """Split contexts integrate in FP32 (FP64 sums): sigma and the per-position
+    maps of ComputeSigmasWithImages stay within the split bar of the plain path;
+    the lifetime map (no GetSigma) is the plain one."""
+    w = workloads.config0()
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    plain, split = pair(w, g, cuda_device)
+    temps = [1e-3, 4.0, 40.0]
+    try:
+        for coherent in (True, False):
+            plain.InitSample(g, settings_of(w), coherent)
+            split.InitSample(g, settings_of(w), coherent)
+            for B in (2.0, 20.0):
+                a = plain.ComputeSigmasWithImages(B, temps)
+                b = split.ComputeSigmasWithImages(B, temps)
+                for x, y in zip(a, b):
+                    assert abs(x.result.xx - y.result.xx) <= SPLIT_SIGMA_RTOL * abs(x.result.xx)
+                    assert abs(x.result.xy - y.result.xy) <= SPLIT_SIGMA_RTOL * abs(x.result.xy)
+                    assert np.array_equal(x.particle_lifetimes, y.particle_lifetimes)
+                    for u, v in ((x.xx_buffer, y.xx_buffer), (x.xy_buffer, y.xy_buffer)):
+                        assert np.abs(u - v).max() <= SPLIT_SIGMA_RTOL * np.abs(u).max()
+    finally:
+        plain.close()
+        split.close()
