@@ -482,7 +482,7 @@ def run_ours(args) -> None:
         k = res[name]["kernel"]
         achieved = k["flops"] / (k["ms"] * 1e-3) / 1e12
         return {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak if peak else None, "traffic": profiled_traffic(name),
+                "frac": achieved / peak if peak else None, "traffic": profiled_traffic(name, w.orbits_per_pass),
                 "kernel": "lifetime_split_kernel + lifetime_retrace_kernel" if name == "split" else "lifetime_fp64_kernel",
                 "work": "algorithmic FP64-op count of the reference's TraceOrbit (flop_model) per launch",
                 "peak_source": peak_src, "flop_model": FLOP_MODEL, "per_launch": k["per_launch"],
@@ -907,22 +907,30 @@ def mlp_roofline(q: int, n_nets: int, ms: float) -> dict:
             "note": "latency-bound: a 4096 x 256 x 256 layer is 0.27 GFLOP, a few microseconds at peak"}
 
 
-def profiled_traffic(name: str):
+def profiled_traffic(name: str, orbits: int | None = None):
     """DRAM bytes per launch from a committed ncu summary ("split", "fp64" or a
-    file name under profiles/), if present."""
+    file name under profiles/), if present. With `orbits`, a summary that states
+    the orbits of its captured launch (`orbits_per_launch:`) is scaled to a launch
+    of that many orbits (the lifetime kernels write 8 bytes per orbit and read
+    little else)."""
     if name.endswith(".md"):
         p = ROOT / "profiles" / name
     else:
         p = ROOT / "profiles" / ("lifetime_split_config1.md" if name == "split" else "lifetime_fp64_config1.md")
     if not p.exists():
         return None
+    fields = {}
     for line in p.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
+        for key in ("traffic_bytes_per_launch", "orbits_per_launch"):
+            if line.startswith(key + ":"):
+                try:
+                    fields[key] = float(line.split(":", 1)[1].strip())
+                except ValueError:
+                    pass
+    traffic = fields.get("traffic_bytes_per_launch")
+    if traffic is not None and orbits and fields.get("orbits_per_launch"):
+        traffic *= orbits / fields["orbits_per_launch"]
+    return traffic
 
 
 def main() -> None:
