@@ -55,6 +55,7 @@ struct es_ctx {
     int n_pos = 0;
     double* d_lifetimes = nullptr;
     es::PhaseOrbit* d_phase_orbit = nullptr;
+    double4* d_orbit_table = nullptr;  // split precision: the pass's per-phase orbit table
     es::PhaseSigma* d_phase_sigma = nullptr;
     unsigned long long* d_metrics = nullptr;
     int* d_error = nullptr;
@@ -162,6 +163,7 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.retrace = ctx->d_retrace;
     L.retrace_count = ctx->d_retrace_count;
     L.retrace_cap = ctx->retrace_cap;
+    L.orbit_table = ctx->d_orbit_table;
     return L;
 }
 
@@ -174,7 +176,7 @@ es_status enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
         make_launch(ctx, magnetic_field, ctx->settings.particle_speed, ctx->settings.is_clockwise ? 1 : 0, ctx->coherent);
     if (ctx->desc.precision == ES_PRECISION_SPLIT) {
         ES_CUDA(es::launch_lifetimes_split(L, ctx->stream), "split lifetime kernel launch");
-        ctx->launches += 2;
+        ctx->launches += 3;  // orbit table, lifetime walk, FP64 re-trace
     } else {
         ES_CUDA(es::launch_lifetimes_fp64(L, ctx->stream), "lifetime kernel launch");
         ctx->launches++;
@@ -283,6 +285,7 @@ void release(es_ctx* ctx)
     cudaFree(ctx->d_cell_end);
     cudaFree(ctx->d_lifetimes);
     cudaFree(ctx->d_phase_orbit);
+    cudaFree(ctx->d_orbit_table);
     cudaFree(ctx->d_phase_sigma);
     cudaFree(ctx->d_metrics);
     cudaFree(ctx->d_error);
@@ -347,6 +350,8 @@ es_status es_create(const es_sim_desc* desc, es_ctx** out)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_lifetimes, sizeof(double) * ctx->n_orbits);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_phase_orbit, sizeof(es::PhaseOrbit) * n_phase);
+    if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT)
+        e = cudaMalloc(&ctx->d_orbit_table, sizeof(double4) * n_phase);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_phase_sigma, sizeof(es::PhaseSigma) * n_phase);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_metrics, sizeof(unsigned long long) * es::kMetCount);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(int));

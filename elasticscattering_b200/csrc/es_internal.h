@@ -65,6 +65,11 @@ struct LifetimeLaunch {
     long long* retrace;           // orbits handed to the FP64 re-trace
     unsigned long long* retrace_count;
     long long retrace_cap;
+    // Per-pass orbit table of the split kernels, [n_phase] x {shift_x, shift_y,
+    // bound_time, phi}: CreateParticle's per-phase quantities at this pass's
+    // radius and w, written by orbit_table_kernel before the lifetime kernel
+    // (null: computed per orbit).
+    double4* orbit_table;
 };
 
 enum LifetimeVariant : int {

@@ -35,6 +35,20 @@ __global__ void __launch_bounds__(256, kMinBlocks) lifetime_split_kernel(Lifetim
     flush_split_metrics(P.metrics, mask, cnt, flags, !retrace);
 }
 
+// The pass's orbit table: per phase, CreateParticle's centre shift and bound
+// time (src/sim/es/lifetime.h:36-58, details.h:243-250) at this pass's radius
+// and w -- the FP64 quotients make_orbit would otherwise form for every orbit.
+__global__ void orbit_table_kernel(LifetimeLaunch P)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= P.n_phase) return;
+    const PhaseOrbit ph = P.phase[v];
+    const double shift_x = (ph.vel_y * P.radius) / P.speed;
+    const double shift_y = (-ph.vel_x * P.radius) / P.speed;
+    const double bound_time = P.coherent ? kINF : ph.bound_dphi / P.w;
+    P.orbit_table[v] = make_double4(shift_x, shift_y, bound_time, ph.phi);
+}
+
 // Exact FP64 re-trace of the listed orbits (grid-stride over the device count).
 __global__ void __launch_bounds__(256, 4) lifetime_retrace_kernel(LifetimeLaunch P)
 {
@@ -67,6 +81,10 @@ cudaError_t launch_lifetimes_split(const LifetimeLaunch& L, cudaStream_t s)
     if (L.n_orbits <= 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(L.retrace_count, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
+    if (L.orbit_table != nullptr) {
+        orbit_table_kernel<<<(unsigned)((L.n_phase + 127) / 128), 128, 0, s>>>(L);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     const long long blocks = (L.n_orbits + 255) / 256;
     lifetime_split_kernel<4><<<(unsigned)blocks, 256, 0, s>>>(L);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -48,6 +48,7 @@ constexpr float kPolarMark = -2.0f;    // crossing value that marks such an edge
 // memory (the batched kernels), loaded where the compiler chooses.
 struct LaunchFields {
     static constexpr bool kCrossOutOfLine = true;  // see first_cross_angle
+    static constexpr bool kOrbitTable = true;      // see make_orbit
     const LifetimeLaunch& P;
     __device__ __forceinline__ const int* cell_end() const { return P.cell_end; }
     __device__ __forceinline__ const float2* imps32() const { return P.imps32; }
@@ -71,10 +72,12 @@ struct LaunchFields {
     __device__ __forceinline__ int clockwise() const { return P.clockwise; }
     __device__ __forceinline__ int coherent() const { return P.coherent; }
     __device__ __forceinline__ int walk_cap() const { return P.walk_cap; }
+    __device__ __forceinline__ const double4* orbit_table() const { return P.orbit_table; }
 };
 
 struct SharedFields {
     static constexpr bool kCrossOutOfLine = false;
+    static constexpr bool kOrbitTable = false;
     const LifetimeLaunch* P;  // shared memory
     __device__ __forceinline__ const int* cell_end() const { return P->cell_end; }
     __device__ __forceinline__ const float2* imps32() const { return P->imps32; }
@@ -98,6 +101,7 @@ struct SharedFields {
     __device__ __forceinline__ int clockwise() const { return P->clockwise; }
     __device__ __forceinline__ int coherent() const { return P->coherent; }
     __device__ __forceinline__ int walk_cap() const { return P->walk_cap; }
+    __device__ __forceinline__ const double4* orbit_table() const { return nullptr; }
 };
 
 __device__ __forceinline__ float wrap2pi(float a) { return a - kTwoPiF * floorf(a * (1.0f / kTwoPiF)); }
@@ -550,11 +554,20 @@ __device__ __forceinline__ OrbitD make_orbit(const F& f, long long g, dv2& pos)
     const int i = (int)(pidx % f.dim());
     const int j = (int)(pidx / f.dim());
     pos = dv2{(double)i * f.dist() + f.off_x(), (double)j * f.dist() + f.off_y()};
-    const PhaseOrbit ph = f.phase()[v];
     OrbitD o;
     o.radius = f.radius();
     o.radius_sq = f.radius_sq();
     o.clockwise = f.clockwise() != 0;
+    if (F::kOrbitTable && f.orbit_table() != nullptr) {
+        // the pass's table holds the same FP64 quotients (orbit_table_kernel)
+        const double2* t = reinterpret_cast<const double2*>(f.orbit_table() + v);
+        const double2 shift = __ldg(t), rest = __ldg(t + 1);  // (shift_x, shift_y), (bound_time, phi)
+        o.center = o.clockwise ? dv2{pos.x - shift.x, pos.y - shift.y} : dv2{pos.x + shift.x, pos.y + shift.y};
+        o.bound_time = rest.x;
+        o.particle_angle = rest.y;
+        return o;
+    }
+    const PhaseOrbit ph = f.phase()[v];
     const double shift_x = (ph.vel_y * o.radius) / f.speed();
     const double shift_y = (-ph.vel_x * o.radius) / f.speed();
     o.center = o.clockwise ? dv2{pos.x - shift_x, pos.y - shift_y} : dv2{pos.x + shift_x, pos.y + shift_y};
