@@ -3,8 +3,10 @@
 //
 // No reference counterpart. Architecture 5 -> 256 x 4 -> 2, GELU, one network per
 // ensemble member. The four hidden layers (99.7% of the weights) run on the tensor
-// cores (mma.sync m16n8k16) with BF16 weights and activations and FP32
-// accumulation; the 256 -> 2 output head runs in FP32 on the FP32 master
+// cores with BF16 weights and activations and FP32 accumulation: the forward pass
+// of the three 256 x 256 layers with tcgen05.mma (TMEM accumulators,
+// tc_hidden_kernel), the 5 -> 256 layer and the backward GEMMs with mma.sync
+// m16n8k16 (gemm_kernel); the 256 -> 2 output head runs in FP32 on the FP32 master
 // weights and FP32 activations, because its 256 terms cancel into a small
 // output and BF16 rounding there measurably limited the fit (about 1% error in
 // sigma). FP32 master weights and Adam state. Training and inference are this
@@ -176,6 +178,177 @@ cudaError_t gemm(const GemmArgs& g, int nets, cudaStream_t s)
 {
     const dim3 grid((g.N + kBN - 1) / kBN, (g.M + kBM - 1) / kBM, nets);
     gemm_kernel<TA, TB, EPI><<<grid, 128, 0, s>>>(g);
+    return cudaGetLastError();
+}
+
+// ---- Hidden layers 1-3 (K = N = 256) on the 5th-generation tensor cores ----
+//
+// tc_hidden_kernel: Z = A W^T + b and GELU(Z) for 128 rows x all 256 columns of
+// one member per CTA (grid = row tiles x members), with tcgen05.mma:
+//   - the CTA stages its A tile (128 x 256 BF16, 64 KB) and the member's W
+//     (256 x 256, 128 KB) in shared memory in the no-swizzle K-major layout of
+//     the UMMA descriptors: 8-row x 16-byte core matrices of 128 contiguous
+//     bytes, the K chunks of a row group adjacent (leading byte offset 128 B),
+//     row groups 32 x 128 B apart (stride byte offset 4096 B);
+//   - warp 0 allocates 256 TMEM columns (the 128 x 256 FP32 accumulator); one
+//     thread issues the 16 MMAs of K = 16 (kind::f16, BF16 in, FP32 out,
+//     M = 128, N = 256) and commits them to an mbarrier;
+//   - every warp reads its 32 accumulator lanes (rows) back with tcgen05.ld,
+//     adds the bias, writes Z (FP32) and GELU(Z) (BF16), and warp 0 frees the
+//     TMEM.
+// The wait on the MMAs is bounded: past its limit the kernel records
+// kTcTimeout in *err, waits once more (also bounded) and frees the TMEM, so
+// the caller gets an error instead of a hung device.
+constexpr int kTcM = 128, kTcN = 256, kTcK = 256;
+constexpr int kTcSmemA = kTcM * kTcK * 2, kTcSmemB = kTcN * kTcK * 2;
+constexpr int kTcSmem = kTcSmemA + kTcSmemB;  // 192 KB dynamic shared memory
+constexpr int kTcTimeout = 1;
+constexpr unsigned kTcWaitLimit = 1u << 24;
+
+// UMMA shared-memory descriptor, no swizzle (layout type 0), version 1 (sm_100).
+__device__ __forceinline__ unsigned long long umma_desc(unsigned saddr, unsigned lbo, unsigned sbo)
+{
+    return (unsigned long long)((saddr >> 4) & 0x3FFFu) | ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N >> 3, M >> 4.
+constexpr unsigned kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(kTcN >> 3) << 17) |
+                              ((unsigned)(kTcM >> 4) << 24);
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned addr, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__global__ void __launch_bounds__(128, 1) tc_hidden_kernel(GemmArgs g, int* err)
+{
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ __align__(8) unsigned long long mbar;
+    __shared__ unsigned tmem_base;
+    const int net = blockIdx.y;
+    const int m0 = blockIdx.x * kTcM;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const __nv_bfloat16* A = g.A + net * g.strideA;
+    const __nv_bfloat16* B = g.B + net * g.strideB;
+    const unsigned sA = (unsigned)__cvta_generic_to_shared(tc_smem);
+    const unsigned sB = sA + kTcSmemA;
+    const unsigned sbar = (unsigned)__cvta_generic_to_shared(&mbar);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"((unsigned)__cvta_generic_to_shared(&tmem_base)), "r"(kTcN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(sbar));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    // stage A (rows past M read as zero) and W: 16-byte chunks into core matrices
+    constexpr int kChunks = kTcK / 8;  // 16-byte chunks per row
+    for (int q = tid; q < kTcM * kChunks; q += 128) {
+        const int r = q / kChunks, kc = q % kChunks;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (m0 + r < g.M) v = *reinterpret_cast<const uint4*>(A + (long long)(m0 + r) * g.lda + kc * 8);
+        *reinterpret_cast<uint4*>(tc_smem + ((r >> 3) * kChunks + kc) * 128 + (r & 7) * 16) = v;
+    }
+    for (int q = tid; q < kTcN * kChunks; q += 128) {
+        const int n = q / kChunks, kc = q % kChunks;
+        const uint4 v = *reinterpret_cast<const uint4*>(B + (long long)n * g.ldb + kc * 8);
+        *reinterpret_cast<uint4*>(tc_smem + kTcSmemA + ((n >> 3) * kChunks + kc) * 128 + (n & 7) * 16) = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy stores -> MMA reads
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = tmem_base;
+
+    if (tid == 0) {
+#pragma unroll 1
+        for (int s = 0; s < kTcK / 16; s++) {
+            // K step s covers chunks 2s and 2s + 1 of every row group
+            const unsigned long long da = umma_desc(sA + 2 * s * 128, 128, kChunks * 128);
+            const unsigned long long db = umma_desc(sB + 2 * s * 128, 128, kChunks * 128);
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                :: "r"(tmem), "l"(da), "l"(db), "r"(kTcIdesc), "r"(s));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(sbar) : "memory");
+    }
+    bool done = false;
+    for (unsigned it = 0; it < kTcWaitLimit && !done; it++) done = mbar_try_wait(sbar, 0);
+    if (!done) {
+        atomicOr(err, kTcTimeout);
+        for (unsigned it = 0; it < kTcWaitLimit && !done; it++) done = mbar_try_wait(sbar, 0);
+    }
+    done = __all_sync(0xffffffffu, done);  // tcgen05.ld below is warp-collective
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (done) {
+        // warp w reads accumulator lanes 32w .. 32w + 31 (its rows), 32 columns at a time
+        const int r = warp * 32 + lane;
+        const int m = m0 + r;
+        float* out = g.out + net * g.strideOut;
+        __nv_bfloat16* out2 = g.out2 + net * g.strideOut;
+        const float* bias = g.bias + net * g.strideBias;
+#pragma unroll 1
+        for (int c0 = 0; c0 < kTcN; c0 += 32) {
+            unsigned v[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < g.M) {
+                const long long o = (long long)m * g.N + c0;
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const float z = __uint_as_float(v[j]) + bias[c0 + j];
+                    out[o + j] = z;
+                    out2[o + j] = __float2bfloat16(gelu(z));
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTcN));
+}
+
+// Whether a hidden-layer GEMM can take the tensor-core kernel: K = N = 256,
+// forward (A and W both K-major), 16-byte aligned rows and member strides.
+bool tc_eligible(const GemmArgs& g)
+{
+    const auto al = [](const void* p) { return ((unsigned long long)p & 15ull) == 0; };
+    return g.K == kTcK && g.N == kTcN && g.lda == kTcK && g.ldb == kTcK && al(g.A) && al(g.B) &&
+           (g.strideA * 2) % 16 == 0 && (g.strideB * 2) % 16 == 0 && g.bias && g.out && g.out2;
+}
+
+cudaError_t gemm_hidden_tc(const GemmArgs& g, int nets, int* err, cudaStream_t s)
+{
+    static bool attr_set = false;  // per process; the attribute is per function
+    if (!attr_set) {
+        const cudaError_t e = cudaFuncSetAttribute(tc_hidden_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    tc_hidden_kernel<<<dim3((g.M + kTcM - 1) / kTcM, nets), 128, kTcSmem, s>>>(g, err);
     return cudaGetLastError();
 }
 
@@ -409,6 +582,8 @@ struct es_mlp {
     float* d_dy = nullptr;                   // output gradient [nets][cap][kOut], FP32
     float* d_xin = nullptr;                  // query staging [cap][kIn], FP32
     float* d_loss = nullptr;                 // [nets]
+    int* d_tc_err = nullptr;                 // tc_hidden_kernel's bounded-wait flag
+    int* h_tc_err = nullptr;                 // pinned copy
     float* h_loss = nullptr;                 // pinned
     float* d_mean = nullptr;
     float* d_spread = nullptr;
@@ -498,7 +673,8 @@ cudaError_t forward(es_mlp* m, int rows, bool shared_input)
         g.out = m->d_z[l];
         g.strideOut = (long long)m->cap * N;
         g.out2 = m->d_act[l + 1];
-        e = es::gemm<false, false, es::kEpiHidden>(g, m->nets, m->stream);
+        if (es::tc_eligible(g)) e = es::gemm_hidden_tc(g, m->nets, m->d_tc_err, m->stream);
+        else e = es::gemm<false, false, es::kEpiHidden>(g, m->nets, m->stream);
         m->launches++;
     }
     // the FP32 head
@@ -576,6 +752,16 @@ cudaError_t backward(es_mlp* m, int rows)
     return e;
 }
 
+// The tensor-core kernel's flag (read back with the caller's synchronisation):
+// a bounded wait ran out, so that call's outputs are not valid.
+es_status check_tc(es_mlp* m)
+{
+    if (*m->h_tc_err == 0) return ES_OK;
+    *m->h_tc_err = 0;
+    cudaMemsetAsync(m->d_tc_err, 0, sizeof(int), m->stream);
+    return mfail(m, ES_ERR_TIMEOUT, "tensor-core GEMM: the wait for the MMAs ran out");
+}
+
 es_status bind_mlp(es_mlp* m)
 {
     if (!m) return ES_ERR_BAD_ARG;
@@ -635,6 +821,9 @@ es_status es_mlp_create(int32_t n_nets, int32_t device_ordinal, es_mlp** out)
     if (e == cudaSuccess) e = cudaMalloc(&m->d_w16, sizeof(__nv_bfloat16) * W);
     if (e == cudaSuccess) e = cudaMalloc(&m->d_is_weight, sizeof(int) * P);
     if (e == cudaSuccess) e = cudaMalloc(&m->d_loss, sizeof(float) * n_nets);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_tc_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(m->d_tc_err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&m->h_tc_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&m->h_loss, sizeof(float) * n_nets);
     if (e == cudaSuccess)
         e = cudaMemcpy(m->d_is_weight, is_w.data(), sizeof(int) * P, cudaMemcpyHostToDevice);
@@ -668,6 +857,8 @@ es_status es_mlp_destroy(es_mlp* m)
     cudaFree(m->d_x);
     cudaFree(m->d_y);
     cudaFree(m->d_loss);
+    cudaFree(m->d_tc_err);
+    cudaFreeHost(m->h_tc_err);
     if (m->h_loss) cudaFreeHost(m->h_loss);
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
@@ -757,7 +948,9 @@ es_status es_mlp_train(es_mlp* m, int32_t steps, int32_t batch, float lr, uint64
         ES_MCUDA(cudaMemcpyAsync(m->h_loss, m->d_loss, sizeof(float) * m->nets, cudaMemcpyDeviceToHost, m->stream),
                  "loss readback");
     }
+    ES_MCUDA(cudaMemcpyAsync(m->h_tc_err, m->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, m->stream), "flag readback");
     ES_MCUDA(cudaStreamSynchronize(m->stream), "training");
+    if ((st = check_tc(m)) != ES_OK) return st;
     if (out_loss) std::memcpy(out_loss, m->h_loss, sizeof(float) * m->nets);
     return ES_OK;
 }
@@ -795,7 +988,9 @@ es_status es_mlp_gradients(es_mlp* m, const float* x, const float* y, int32_t ro
              "gradient readback");
     ES_MCUDA(cudaMemcpyAsync(m->h_loss, m->d_loss, sizeof(float) * m->nets, cudaMemcpyDeviceToHost, m->stream),
              "loss readback");
+    ES_MCUDA(cudaMemcpyAsync(m->h_tc_err, m->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, m->stream), "flag readback");
     ES_MCUDA(cudaStreamSynchronize(m->stream), "gradients");
+    if ((st = check_tc(m)) != ES_OK) return st;
     if (out_loss) std::memcpy(out_loss, m->h_loss, sizeof(float) * m->nets);
     return ES_OK;
 }
@@ -839,9 +1034,10 @@ es_status es_mlp_predict(es_mlp* m, const float* x, int64_t q, float* out_each, 
         e = cudaMemcpyAsync(out_mean, m->d_mean, sizeof(float) * q * es::kOut, cudaMemcpyDeviceToHost, m->stream);
     if (e == cudaSuccess && out_spread)
         e = cudaMemcpyAsync(out_spread, m->d_spread, sizeof(float) * q * es::kOut, cudaMemcpyDeviceToHost, m->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_tc_err, m->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, m->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
     ES_MCUDA(e, "surrogate query");
-    return ES_OK;
+    return check_tc(m);
 }
 
 int64_t es_mlp_launch_count(const es_mlp* m) { return m ? m->launches : 0; }
