@@ -184,22 +184,26 @@ cudaError_t gemm(const GemmArgs& g, int nets, cudaStream_t s)
 // ---- Hidden layers 1-3 (K = N = 256) on the 5th-generation tensor cores ----
 //
 // tc_hidden_kernel: Z = A W^T + b and GELU(Z) for 128 rows x all 256 columns of
-// one member per CTA (grid = row tiles x members), with tcgen05.mma:
+// one member per CTA (grid = row tiles x members, 512 threads), with tcgen05.mma:
 //   - the CTA stages its A tile (128 x 256 BF16, 64 KB) and the member's W
-//     (256 x 256, 128 KB) in shared memory in the no-swizzle K-major layout of
+//     (256 x 256, 128 KB, L2-resident: every row tile reads it) with 16-byte
+//     cp.async copies in shared memory in the no-swizzle K-major layout of
 //     the UMMA descriptors: 8-row x 16-byte core matrices of 128 contiguous
 //     bytes, the K chunks of a row group adjacent (leading byte offset 128 B),
 //     row groups 32 x 128 B apart (stride byte offset 4096 B);
 //   - warp 0 allocates 256 TMEM columns (the 128 x 256 FP32 accumulator); one
 //     thread issues the 16 MMAs of K = 16 (kind::f16, BF16 in, FP32 out,
 //     M = 128, N = 256) and commits them to an mbarrier;
-//   - every warp reads its 32 accumulator lanes (rows) back with tcgen05.ld,
-//     adds the bias, writes Z (FP32) and GELU(Z) (BF16), and warp 0 frees the
-//     TMEM.
+//   - 16 warps read the accumulator back with tcgen05.ld (each warp its lane
+//     quarter's rows, a quarter of the columns), add the bias and write Z
+//     (FP32; skipped when out is null) and GELU(Z) (BF16) with 16-byte
+//     stores; warp 0 frees the TMEM. The GELU epilogue (erff per element) is
+//     most of the kernel's instructions, hence the 16 warps.
 // The wait on the MMAs is bounded: past its limit the kernel records
 // kTcTimeout in *err, waits once more (also bounded) and frees the TMEM, so
 // the caller gets an error instead of a hung device.
 constexpr int kTcM = 128, kTcN = 256, kTcK = 256;
+constexpr int kTcThreads = 512;  // 16 warps: warp w reads TMEM lanes 32 (w % 4).., columns 64 (w / 4)..
 constexpr int kTcSmemA = kTcM * kTcK * 2, kTcSmemB = kTcN * kTcK * 2;
 constexpr int kTcSmem = kTcSmemA + kTcSmemB;  // 192 KB dynamic shared memory
 constexpr int kTcTimeout = 1;
@@ -229,7 +233,7 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned addr, unsigned parity)
     return ok != 0;
 }
 
-__global__ void __launch_bounds__(128, 1) tc_hidden_kernel(GemmArgs g, int* err)
+__global__ void __launch_bounds__(kTcThreads, 1) tc_hidden_kernel(GemmArgs g, int* err)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ __align__(8) unsigned long long mbar;
@@ -252,20 +256,27 @@ __global__ void __launch_bounds__(128, 1) tc_hidden_kernel(GemmArgs g, int* err)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(sbar));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    // stage A (rows past M read as zero) and W: 16-byte chunks into core matrices
+    // Stage A (rows past M are zero-filled) and W: 16-byte cp.async copies into
+    // the core matrices, all of a thread's 96 copies in flight at once (a
+    // load-then-store loop would wait out one global-load latency per chunk).
     constexpr int kChunks = kTcK / 8;  // 16-byte chunks per row
-    for (int q = tid; q < kTcM * kChunks; q += 128) {
+    for (int q = tid; q < kTcM * kChunks; q += kTcThreads) {
         const int r = q / kChunks, kc = q % kChunks;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (m0 + r < g.M) v = *reinterpret_cast<const uint4*>(A + (long long)(m0 + r) * g.lda + kc * 8);
-        *reinterpret_cast<uint4*>(tc_smem + ((r >> 3) * kChunks + kc) * 128 + (r & 7) * 16) = v;
+        const bool in = m0 + r < g.M;
+        const __nv_bfloat16* src = A + (long long)(in ? m0 + r : 0) * g.lda + kc * 8;
+        const unsigned dst = sA + ((r >> 3) * kChunks + kc) * 128 + (r & 7) * 16;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(dst), "l"(src), "r"(in ? 16 : 0)
+                     : "memory");
     }
-    for (int q = tid; q < kTcN * kChunks; q += 128) {
+    for (int q = tid; q < kTcN * kChunks; q += kTcThreads) {
         const int n = q / kChunks, kc = q % kChunks;
-        const uint4 v = *reinterpret_cast<const uint4*>(B + (long long)n * g.ldb + kc * 8);
-        *reinterpret_cast<uint4*>(tc_smem + kTcSmemA + ((n >> 3) * kChunks + kc) * 128 + (n & 7) * 16) = v;
+        const unsigned dst = sB + ((n >> 3) * kChunks + kc) * 128 + (n & 7) * 16;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(B + (long long)n * g.ldb + kc * 8)
+                     : "memory");
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy stores -> MMA reads
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy writes -> MMA reads
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -296,14 +307,18 @@ __global__ void __launch_bounds__(128, 1) tc_hidden_kernel(GemmArgs g, int* err)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
     if (done) {
-        // warp w reads accumulator lanes 32w .. 32w + 31 (its rows), 32 columns at a time
-        const int r = warp * 32 + lane;
-        const int m = m0 + r;
-        float* out = g.out + net * g.strideOut;
+        // Warp w may read only TMEM lanes 32 (w % 4) .. + 31: its rows. The four
+        // warps of a lane quarter split the 256 columns, 64 each, read 32 at a
+        // time; a thread holds 32 columns of its row and writes them with
+        // 16-byte stores (Z skipped when out is null).
+        const int quarter = warp & 3;
+        const int col0 = (warp >> 2) * 64;
+        const int m = m0 + quarter * 32 + lane;
+        float* out = g.out ? g.out + net * g.strideOut : nullptr;
         __nv_bfloat16* out2 = g.out2 + net * g.strideOut;
         const float* bias = g.bias + net * g.strideBias;
 #pragma unroll 1
-        for (int c0 = 0; c0 < kTcN; c0 += 32) {
+        for (int c0 = col0; c0 < col0 + 64; c0 += 32) {
             unsigned v[32];
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -313,15 +328,26 @@ __global__ void __launch_bounds__(128, 1) tc_hidden_kernel(GemmArgs g, int* err)
                   "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
                   "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
                   "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                : "r"(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0));
+                : "r"(tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (m < g.M) {
                 const long long o = (long long)m * g.N + c0;
 #pragma unroll
-                for (int j = 0; j < 32; j++) {
-                    const float z = __uint_as_float(v[j]) + bias[c0 + j];
-                    out[o + j] = z;
-                    out2[o + j] = __float2bfloat16(gelu(z));
+                for (int j = 0; j < 32; j += 8) {
+                    float z[8];
+                    unsigned h[4];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) z[u] = __uint_as_float(v[j + u]) + bias[c0 + j + u];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const __nv_bfloat162 pr = __floats2bfloat162_rn(gelu(z[2 * u]), gelu(z[2 * u + 1]));
+                        h[u] = *reinterpret_cast<const unsigned*>(&pr);
+                    }
+                    if (out) {
+                        *reinterpret_cast<float4*>(out + o + j) = make_float4(z[0], z[1], z[2], z[3]);
+                        *reinterpret_cast<float4*>(out + o + j + 4) = make_float4(z[4], z[5], z[6], z[7]);
+                    }
+                    *reinterpret_cast<uint4*>(out2 + o + j) = make_uint4(h[0], h[1], h[2], h[3]);
                 }
             }
         }
@@ -332,12 +358,14 @@ __global__ void __launch_bounds__(128, 1) tc_hidden_kernel(GemmArgs g, int* err)
 }
 
 // Whether a hidden-layer GEMM can take the tensor-core kernel: K = N = 256,
-// forward (A and W both K-major), 16-byte aligned rows and member strides.
+// forward (A and W both K-major), 16-byte aligned rows and member strides of
+// the operands and of the outputs (its 16-byte stores).
 bool tc_eligible(const GemmArgs& g)
 {
     const auto al = [](const void* p) { return ((unsigned long long)p & 15ull) == 0; };
     return g.K == kTcK && g.N == kTcN && g.lda == kTcK && g.ldb == kTcK && al(g.A) && al(g.B) &&
-           (g.strideA * 2) % 16 == 0 && (g.strideB * 2) % 16 == 0 && g.bias && g.out && g.out2;
+           (g.strideA * 2) % 16 == 0 && (g.strideB * 2) % 16 == 0 && g.bias && g.out2 && al(g.out2) &&
+           (g.out == nullptr || al(g.out)) && g.strideOut % 8 == 0;
 }
 
 cudaError_t gemm_hidden_tc(const GemmArgs& g, int nets, int* err, cudaStream_t s)
@@ -348,7 +376,7 @@ cudaError_t gemm_hidden_tc(const GemmArgs& g, int nets, int* err, cudaStream_t s
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    tc_hidden_kernel<<<dim3((g.M + kTcM - 1) / kTcM, nets), 128, kTcSmem, s>>>(g, err);
+    tc_hidden_kernel<<<dim3((g.M + kTcM - 1) / kTcM, nets), kTcThreads, kTcSmem, s>>>(g, err);
     return cudaGetLastError();
 }
 
@@ -650,7 +678,10 @@ es::GemmArgs args0() { return es::GemmArgs{}; }
 
 // Forward pass of every member on rows already staged in d_act[0] (BF16
 // [nets][rows][kIn], or [rows][kIn] shared when shared_input).
-cudaError_t forward(es_mlp* m, int rows, bool shared_input)
+// keep_z: write every hidden layer's pre-activation Z (FP32), which the
+// backward pass reads; a query pass (false) writes only the last one, the
+// head's input.
+cudaError_t forward(es_mlp* m, int rows, bool shared_input, bool keep_z)
 {
     const Layout& L = layout();
     const long long P = L.n_params, W = L.n_weights;
@@ -670,9 +701,11 @@ cudaError_t forward(es_mlp* m, int rows, bool shared_input)
         g.K = K;
         g.bias = m->d_p + L.b_off[l];
         g.strideBias = P;
-        g.out = m->d_z[l];
         g.strideOut = (long long)m->cap * N;
         g.out2 = m->d_act[l + 1];
+        g.out = m->d_z[l];
+        // only the tensor-core kernel can skip Z
+        if (!keep_z && l + 2 < es::kLayers && es::tc_eligible(g)) g.out = nullptr;
         if (es::tc_eligible(g)) e = es::gemm_hidden_tc(g, m->nets, m->d_tc_err, m->stream);
         else e = es::gemm<false, false, es::kEpiHidden>(g, m->nets, m->stream);
         m->launches++;
@@ -772,7 +805,7 @@ es_status bind_mlp(es_mlp* m)
 // Loss and gradients on the staged minibatch (d_act[0], d_yb).
 es_status loss_and_grads(es_mlp* m, int rows)
 {
-    cudaError_t e = forward(m, rows, false);
+    cudaError_t e = forward(m, rows, false, true);
     if (e == cudaSuccess) {
         es::loss_kernel<<<m->nets, 256, 0, m->stream>>>(m->d_z[es::kLayers - 1], m->d_yb, rows, m->cap, m->d_dy,
                                                         m->d_loss);
@@ -1008,7 +1041,7 @@ es_status es_mlp_predict(es_mlp* m, const float* x, int64_t q, float* out_each, 
         m->launches++;
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = forward(m, (int)q, true);
+    if (e == cudaSuccess) e = forward(m, (int)q, true, false);
     if (e == cudaSuccess) {
         // outputs of member k are at d_z[last] + k * cap * kOut; pack them with stride q
         if (m->cap != q) {
