@@ -238,11 +238,13 @@ __device__ __forceinline__ double first_cross_angle(const OrbitD& o, dv2 ip, dou
     return first_cross_angle_open(o, ip, ir);
 }
 
-enum SplitOutcome : int { kSplitDone = 0, kSplitRetrace = 1 };
-
 struct SplitCounters {
     int cells, imps, crossings, start_tests;
 };
+
+// kSplitHit: the walk found its winning disk (and a near-equal runner-up);
+// the FP64 time of the crossing is still to be computed (finish_hit).
+enum SplitOutcome : int { kSplitDone = 0, kSplitRetrace = 1, kSplitHit = 2 };
 
 // The winning disk's reference time (FP64) and the bound clamp.
 template <class F>
@@ -264,10 +266,13 @@ __device__ __forceinline__ double finish_hit(const F& f, const OrbitD& o, int wi
 }
 
 // FP32 walk of one orbit. Returns kSplitDone with `out` set (and flags for the
-// metrics), or kSplitRetrace when the orbit must be re-traced in FP64.
-template <class F>
+// metrics), or kSplitRetrace when the orbit must be re-traced in FP64. With
+// kDefer it returns kSplitHit instead of computing the winner's FP64 time: the
+// winning disk in win.x, a near-equal second in win.y (else -1), for
+// finish_hit.
+template <class F, bool kDefer = false>
 __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos, SplitCounters& cnt, int& flags,
-                                           double& out)
+                                           double& out, int2& win)
 {
     const double r64 = o.radius;
     const double ir64 = f.imp_radius();
@@ -538,6 +543,10 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
         // crossings the geometry accepts: clockwise in the final visit,
         // counter-clockwise in the first. The FP64 walk reproduces that.
         if (o.particle_angle < 0.0 && (o.clockwise ? final_visit : entry_line < 0)) return kSplitRetrace;
+        if constexpr (kDefer) {
+            win = make_int2(k1st, v2 < v1 + kGuard ? k2nd : -1);
+            return kSplitHit;
+        }
         out = finish_hit(f, o, k1st, v2 < v1 + kGuard ? k2nd : -1, flags);
         if (out != out) return kSplitRetrace;  // the winner's crossing point is one the reference drops
         return kSplitDone;
@@ -597,7 +606,46 @@ __device__ __forceinline__ bool split_orbit(const F& f, long long g, SplitCounte
         atomicOr(f.error(), kErrStartCell);
         return false;
     }
-    if (trace_split(f, o, pos, cnt, flags, lt) == kSplitRetrace) {
+    int2 win;
+    if (trace_split(f, o, pos, cnt, flags, lt, win) == kSplitRetrace) {
+        cnt = SplitCounters{0, 0, 0, 0};
+        flags = kTraceOk;
+        return true;
+    }
+    return false;
+}
+
+// split_orbit with the winner's FP64 time taken after a warp sync. `mask`
+// names the lanes of the warp that call this for one orbit each. Lanes end
+// their walks after different numbers of cell steps; they meet at a __syncwarp
+// before the FP64 winner recompute, so that code (sqrt, asin and divisions of
+// the reference's GetCrossPoints/GetAngle) runs once per warp instead of once
+// per distinct exit step: 3% faster per config-1 pass on B200 in the
+// single-pass kernel. Every lane reaches the sync: the walk is bounded by the
+// walk cap and every path returns. The batched kernels keep split_orbit (the
+// deferred form measured 7% slower there, where the orbit's integrand follows
+// the walk in the same kernel).
+template <class F>
+__device__ __forceinline__ bool split_orbit_synced(const F& f, long long g, unsigned mask, SplitCounters& cnt,
+                                                   int& flags, double& lt)
+{
+    dv2 pos;
+    const OrbitD o = make_orbit(f, g, pos);
+    cnt = SplitCounters{0, 0, 0, 0};
+    flags = kTraceOk;
+    lt = 0.0;
+    int st = kSplitDone;
+    int2 win = make_int2(-1, -1);
+    const int cx = (int)((pos.x - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
+    const int cy = (int)((pos.y - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
+    if (cx < 0 || cy < 0 || cx >= f.cpr() || cy >= f.cpr()) atomicOr(f.error(), kErrStartCell);
+    else st = trace_split<F, true>(f, o, pos, cnt, flags, lt, win);
+    __syncwarp(mask);
+    if (st == kSplitHit) {
+        lt = finish_hit(f, o, win.x, win.y, flags);
+        st = (lt != lt) ? kSplitRetrace : kSplitDone;  // NaN: a crossing point the reference drops
+    }
+    if (st == kSplitRetrace) {
         cnt = SplitCounters{0, 0, 0, 0};
         flags = kTraceOk;
         return true;
