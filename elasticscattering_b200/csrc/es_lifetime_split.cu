@@ -49,13 +49,18 @@ __global__ void orbit_table_kernel(LifetimeLaunch P)
     P.orbit_table[v] = make_double4(shift_x, shift_y, bound_time, ph.phi);
 }
 
-// Exact FP64 re-trace of the listed orbits (grid-stride over the device count).
+// Exact FP64 re-trace of the listed orbits (the list length is a device count).
+// The list is short (0.01-0.2 % of a pass) and each entry is a long FP64 walk,
+// so entries go to warps first: entry e runs in warp e mod W (W = the grid's
+// warps), lane (e / W) mod 32. A list of a few thousand orbits then spreads
+// over every SM, one walk per warp, instead of filling the first few blocks.
 __global__ void __launch_bounds__(256, 4) lifetime_retrace_kernel(LifetimeLaunch P)
 {
     const unsigned long long n_list = min(*P.retrace_count, (unsigned long long)P.retrace_cap);
-    for (unsigned long long idx = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n_list;
-         idx += (unsigned long long)gridDim.x * blockDim.x)
-        retrace_orbit(P, P.retrace[idx]);
+    const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x / 32);
+    const unsigned long long wid = (unsigned long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const unsigned long long lane = threadIdx.x & 31;
+    for (unsigned long long e = lane * warps + wid; e < n_list; e += 32 * warps) retrace_orbit(P, P.retrace[e]);
 }
 
 // Cell-local FP32 copy of the ordered impurities: x - (start + cx L), y - (start + cy L).

@@ -558,10 +558,21 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
 template <class F>
 __device__ __forceinline__ OrbitD make_orbit(const F& f, long long g, dv2& pos)
 {
-    const int v = (int)(g % f.n_phase());
-    const long long pidx = g / f.n_phase();
-    const int i = (int)(pidx % f.dim());
-    const int j = (int)(pidx / f.dim());
+    int v, i, j;
+    if (F::kOrbitTable && (unsigned long long)g < (1ull << 32)) {
+        // 32-bit index arithmetic (every pass below 2^32 orbits): a 64-bit
+        // division by a run-time divisor is a long instruction sequence
+        const unsigned g32 = (unsigned)g, np = (unsigned)f.n_phase(), d = (unsigned)f.dim();
+        const unsigned pidx = g32 / np;
+        v = (int)(g32 - pidx * np);
+        i = (int)(pidx % d);
+        j = (int)(pidx / d);
+    } else {
+        v = (int)(g % f.n_phase());
+        const long long pidx = g / f.n_phase();
+        i = (int)(pidx % f.dim());
+        j = (int)(pidx / f.dim());
+    }
     pos = dv2{(double)i * f.dist() + f.off_x(), (double)j * f.dist() + f.off_y()};
     OrbitD o;
     o.radius = f.radius();
