@@ -11,7 +11,11 @@
 namespace es {
 namespace {
 
-template <int kMinBlocks>
+// kDefer: the winner's FP64 time after a warp sync (split_orbit_synced), for
+// passes whose walks end after differing numbers of cell steps; otherwise
+// inside the walk (split_orbit), for passes where nearly every walk ends in
+// its first cell, where the synced form only adds register pressure.
+template <int kMinBlocks, bool kDefer>
 __global__ void __launch_bounds__(256, kMinBlocks) lifetime_split_kernel(LifetimeLaunch P)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -23,7 +27,8 @@ __global__ void __launch_bounds__(256, kMinBlocks) lifetime_split_kernel(Lifetim
     SplitCounters cnt;
     int flags;
     double lt;
-    const bool retrace = split_orbit_synced(LaunchFields{P}, g, mask, cnt, flags, lt);
+    const bool retrace = kDefer ? split_orbit_synced(LaunchFields{P}, g, mask, cnt, flags, lt)
+                                : split_orbit(LaunchFields{P}, g, cnt, flags, lt);
     if (retrace) {
         const unsigned long long slot = atomicAdd(P.retrace_count, 1ull);
         if (slot < (unsigned long long)P.retrace_cap) P.retrace[slot] = g;
@@ -81,7 +86,7 @@ __global__ void local_impurities_kernel(const double2* imps, const int* cell_end
 
 }  // namespace
 
-cudaError_t launch_lifetimes_split(const LifetimeLaunch& L, cudaStream_t s)
+cudaError_t launch_lifetimes_split(const LifetimeLaunch& L, bool defer_finish, cudaStream_t s)
 {
     if (L.n_orbits <= 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(L.retrace_count, 0, sizeof(unsigned long long), s);
@@ -91,7 +96,8 @@ cudaError_t launch_lifetimes_split(const LifetimeLaunch& L, cudaStream_t s)
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     const long long blocks = (L.n_orbits + 255) / 256;
-    lifetime_split_kernel<4><<<(unsigned)blocks, 256, 0, s>>>(L);
+    if (defer_finish) lifetime_split_kernel<4, true><<<(unsigned)blocks, 256, 0, s>>>(L);
+    else lifetime_split_kernel<4, false><<<(unsigned)blocks, 256, 0, s>>>(L);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     lifetime_retrace_kernel<<<148 * 4, 256, 0, s>>>(L);
     return cudaGetLastError();
