@@ -486,7 +486,8 @@ def run_ours(args) -> None:
                 "kernel": "lifetime_split_kernel + lifetime_retrace_kernel" if name == "split" else "lifetime_fp64_kernel",
                 "work": "algorithmic FP64-op count of the reference's TraceOrbit (flop_model) per launch",
                 "peak_source": peak_src, "flop_model": FLOP_MODEL, "per_launch": k["per_launch"],
-                "avg_launch_ms": k["ms"] / len(k["per_launch"]), "retraced_fp64": k["retraced_fp64"]}
+                "avg_launch_ms": k["ms"] / len(k["per_launch"]), "retraced_fp64": k["retraced_fp64"],
+                "issue": profiled_issue(name)}
 
     head = res[args.precision]
     other = "fp64" if args.precision == "split" else "split"
@@ -902,9 +903,34 @@ def mlp_roofline(q: int, n_nets: int, ms: float) -> dict:
         peak = 1590.0
     achieved = flops / (ms * 1e-3) / 1e12
     return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "gemm_kernel (BF16 mma.sync, FP32 accumulate) + head_forward_kernel",
+            "traffic": None,
+            "kernel": "tc_hidden_kernel (tcgen05.mma, BF16 in, FP32 accumulator in TMEM) for the 256 x 256 layers, "
+                      "gemm_kernel (mma.sync) for the 5 -> 256 layer, head_forward_kernel (FP32)",
             "work": f"{flops:.3g} flops per {q}-query batch, {n_nets} members", "peak_source": src,
             "note": "latency-bound: a 4096 x 256 x 256 layer is 0.27 GFLOP, a few microseconds at peak"}
+
+
+def profiled_issue(name: str):
+    """The issue-slot view of a lifetime kernel from its committed ncu summary:
+    the fraction of cycles a warp scheduler issued (smsp__issue_active) and the
+    active lanes per issued instruction. These kernels are issue-bound, so their
+    ceiling is the issue rate with 32 lanes per instruction, not an FMA pipe."""
+    p = ROOT / "profiles" / ("lifetime_split_config1.md" if name == "split" else "lifetime_fp64_config1.md")
+    if not p.exists():
+        return None
+    out = {}
+    for line in p.read_text().splitlines():
+        for key in ("issue_active_frac", "threads_per_instruction"):
+            if line.startswith(key + ":"):
+                try:
+                    out[key] = float(line.split(":", 1)[1].strip())
+                except ValueError:
+                    pass
+    if len(out) != 2:
+        return None
+    out["lane_frac"] = out["threads_per_instruction"] / 32.0
+    out["source"] = f"ncu --set full summary, profiles/{p.name} (config-1 pass, B = 20 T)"
+    return out
 
 
 def profiled_traffic(name: str, orbits: int | None = None):
