@@ -454,7 +454,8 @@ def run_ours(args) -> None:
     batched = {"ms_per_step": float(np.mean(bms)), "value": orbits_per_step / (float(np.mean(bms)) * 1e-3),
                "sigma_points_per_sec": len(w.fields) * n_t / (float(np.mean(bms)) * 1e-3),
                "max_rel_sigma_vs_fp64": float((np.abs(b_sig - f_sig) / np.abs(f_sig)).max()),
-               "note": "es_batch persistent kernel + FP64 re-trace kernel, one graph replay per step"}
+               "note": "es_batch in its default mode (ES_BATCH_PASS_KERNELS: the single-pass kernels for each "
+                       "pass in turn), one graph replay per step"}
 
     peak64 = C.c_double(0.0)
     peak32 = C.c_double(0.0)
@@ -644,7 +645,11 @@ def run_batched(args) -> None:
     total_ms = float(t.item())
     orbits = bs.total_orbits
     points = len(wl.samples) * len(wl.fields) * len(wl.temperatures)
-    kernels_per_replay = (n_pass if tune.shape["mode"] == N.ES_BATCH_PASS_NODES else 1) + 1
+    if tune.shape["mode"] == N.ES_BATCH_PASS_KERNELS:
+        # per pass: orbit table, lifetime walk, FP64 re-trace, integration, reduction
+        kernels_per_replay = 5 * n_pass
+    else:
+        kernels_per_replay = (n_pass if tune.shape["mode"] == N.ES_BATCH_PASS_NODES else 1) + 1
     alg_flops = sum(lifetime_flops(m, 0) for m in mets) + FLOP_MODEL["per_orbit"] * orbits
     retraced = sum(m["retraced_fp64"] for m in mets)
 
@@ -763,7 +768,9 @@ def run_batched(args) -> None:
         "roofline": {"bound": "fp32 pipe", "achieved": achieved, "peak": peak32.value, "unit": "TFLOP/s",
                      "frac": achieved / peak32.value if peak32.value else None,
                      "peak_source": "measured FP32 FMA rate (es_probe_fp32_fma)",
-                     "traffic": profiled_traffic("batch_kernel_config2.md"),
+                     "traffic": (profiled_traffic("split", orbits)
+                                 if tune.shape["mode"] == N.ES_BATCH_PASS_KERNELS
+                                 else profiled_traffic("batch_kernel_config2.md")),
                      "note": "algorithmic FP64-op model of TraceOrbit over the whole graph replay"},
         "split_vs_fp64": {"results": int(rel.size), "max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
                           "above_1e-6": int((rel > 1e-6).sum()), "sigma_points_max_rel": float(prel.max()),

@@ -1,12 +1,14 @@
-"""Batched sweeps: many (sample, field, sector) passes in one persistent kernel.
+"""Batched sweeps: many (sample, field, sector) passes in one graph replay.
 
 The reference runs a sweep as nested loops (SimulationRunner::RunSample,
 src/SimulationRunner.cpp:86-151): per sample one Grid, per field and sector one
 Simulation::ComputeSigmas call. `BatchSweep` takes the whole list of those calls
-at once and runs them through the es_batch_* C ABI (include/es_cuda.h): one
-persistent kernel, recorded once as a CUDA graph and replayed, with stages (b)
-and (c) fused into the lifetime kernel. Each pass returns what
-ComputeSigmas returns for it (one Sigma per temperature) plus its metrics.
+at once and runs them through the es_batch_* C ABI (include/es_cuda.h),
+recorded once as a CUDA graph and replayed. The default mode
+(ES_BATCH_PASS_KERNELS) runs the single-pass kernels for each pass in turn; the
+other modes fuse stages (b) and (c) into one lifetime kernel over all passes
+(ES_BATCH_PERSISTENT and the rest). Each pass returns what ComputeSigmas
+returns for it (one Sigma per temperature) plus its metrics.
 """
 from __future__ import annotations
 
@@ -75,7 +77,7 @@ class BatchSweep:
     """Owner of one es_batch (device buffers, stream, recorded graph)."""
 
     def __init__(self, device: int = 0, chunk_iters: int = 32, blocks_per_sm: int = 4,
-                 precision: int = N.ES_PRECISION_SPLIT, mode: int = N.ES_BATCH_PERSISTENT):
+                 precision: int = N.ES_PRECISION_SPLIT, mode: int = N.ES_BATCH_PASS_KERNELS):
         lib = N.cuda_lib()
         h = C.c_void_p()
         st = lib.es_batch_create(int(device), C.byref(h))

@@ -1,5 +1,13 @@
 // es_batch.cu - batched sweeps: many (sample, field, sector) passes, each with
-// its own temperature list, in one persistent kernel replayed from a CUDA graph.
+// its own temperature list, in one replay of a CUDA graph.
+//
+// Modes (es_batch_mode). ES_BATCH_PASS_KERNELS, the default, records for each
+// pass in turn the single-pass path's kernels (es_lifetime_split.cu or
+// es_lifetime_fp64.cu, then es_integrate.cu) on shared device scratch: the
+// lean lifetime kernel without the integrand is 12-16% faster on B200 than the
+// fused kernels below, and the 16 bytes per orbit it moves through HBM are ~1%
+// of its time. The other modes fuse stages (b) and (c) into the lifetime
+// kernel, as described next.
 //
 // No reference counterpart: the reference runs one pass at a time
 // (SimulationRunner::RunSample, src/SimulationRunner.cpp:103-151, calling
@@ -627,8 +635,9 @@ struct es_batch {
     cudaStream_t stream = nullptr;
     char err[512] = "";
     int64_t launches = 0;
-    // measured best on B200 for config-1-sized passes (the autotuner may choose otherwise)
-    es_batch_tuning tuning{32, 4, ES_PRECISION_SPLIT, ES_BATCH_PERSISTENT};
+    // measured best on B200 for config-1- and config-2-sized passes (12-16% ahead of
+    // ES_BATCH_PERSISTENT on 129^2 to 513^2 start grids; the autotuner may choose otherwise)
+    es_batch_tuning tuning{32, 4, ES_PRECISION_SPLIT, ES_BATCH_PASS_KERNELS};
     int64_t captured_items = -1;              // grid size recorded in the graph (ES_BATCH_GRID)
     static constexpr int kBranches = 8;       // parallel graph branches (ES_BATCH_PASS_NODES)
     cudaStream_t branch[kBranches] = {};
@@ -666,6 +675,17 @@ struct es_batch {
     unsigned long long* d_retrace_count = nullptr;
     unsigned long long* h_retrace_count = nullptr;  // pinned
     int64_t retrace_regrows = 0;
+
+    // ES_BATCH_PASS_KERNELS: per-pass sigma (cap * 2 * kBatchMaxTau doubles, one
+    // slot per distinct tau) and the scratch the single-pass kernels share
+    double* d_psigma = nullptr;
+    double* h_psigma = nullptr;                // pinned
+    double* d_lt = nullptr;                    // one pass's lifetimes
+    long long lt_cap = 0;
+    double4* d_otab = nullptr;                 // one pass's orbit table (split)
+    long long otab_cap = 0;
+    double* d_partial = nullptr;               // integration block partials
+    std::vector<double> pass_phi_factor;       // per kernel position: the sector's phi_integrand_factor
 
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -713,9 +733,23 @@ void free_tables(es_batch* b)
     if (b->h_table) cudaFreeHost(b->h_table);
     if (b->h_acc) cudaFreeHost(b->h_acc);
     if (b->h_metrics) cudaFreeHost(b->h_metrics);
+    cudaFree(b->d_psigma);
+    if (b->h_psigma) cudaFreeHost(b->h_psigma);
     b->d_table = b->h_table = nullptr;
     b->d_acc = b->d_metrics = b->h_acc = b->h_metrics = nullptr;
+    b->d_psigma = b->h_psigma = nullptr;
     b->cap = 0;
+}
+
+void free_pass_scratch(es_batch* b)
+{
+    cudaFree(b->d_lt);
+    cudaFree(b->d_otab);
+    cudaFree(b->d_partial);
+    b->d_lt = nullptr;
+    b->d_otab = nullptr;
+    b->d_partial = nullptr;
+    b->lt_cap = b->otab_cap = 0;
 }
 
 void free_grids(es_batch* b)
@@ -748,6 +782,8 @@ es_status ensure_capacity(es_batch* b, int64_t n)
     ES_BCUDA(cudaMalloc(&b->d_metrics, sizeof(unsigned long long) * es::kMetCount * cap), "batch metrics");
     ES_BCUDA(cudaMallocHost(&b->h_acc, sizeof(unsigned long long) * 2 * es::kBatchMaxTau * cap), "batch accumulators");
     ES_BCUDA(cudaMallocHost(&b->h_metrics, sizeof(unsigned long long) * es::kMetCount * cap), "batch metrics");
+    ES_BCUDA(cudaMalloc(&b->d_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap), "per-pass sigma");
+    ES_BCUDA(cudaMallocHost(&b->h_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap), "per-pass sigma (host)");
     std::memset(b->h_table, 0, b->table_bytes);
     b->cap = cap;
     return ES_OK;
@@ -783,11 +819,87 @@ cudaError_t record_pass_nodes(es_batch* b, const es::BatchLaunch& L)
     return e;
 }
 
+// ES_BATCH_PASS_KERNELS: scratch for the largest pass (allocated before the
+// capture; the graph records the addresses).
+es_status ensure_pass_scratch(es_batch* b)
+{
+    const es::BatchInstanceD* hi = reinterpret_cast<const es::BatchInstanceD*>(b->h_table + b->inst_offset);
+    long long max_orbits = 1, max_phase = 1;
+    for (size_t pos = 0; pos < b->inst.size(); pos++) {
+        max_orbits = std::max(max_orbits, hi[pos].L.n_orbits);
+        max_phase = std::max(max_phase, (long long)hi[pos].L.n_phase);
+    }
+    if (max_orbits <= b->lt_cap && max_phase <= b->otab_cap && b->d_partial) return ES_OK;
+    drop_graph(b);
+    free_pass_scratch(b);
+    ES_BCUDA(cudaMalloc(&b->d_lt, sizeof(double) * (size_t)max_orbits), "pass lifetimes");
+    ES_BCUDA(cudaMalloc(&b->d_otab, sizeof(double4) * (size_t)max_phase), "pass orbit table");
+    ES_BCUDA(cudaMalloc(&b->d_partial, sizeof(double) * 2 * es::kMaxTChunk * es::kIntegrateBlocks),
+             "integration partials");
+    b->lt_cap = max_orbits;
+    b->otab_cap = max_phase;
+    return ES_OK;
+}
+
+// ES_BATCH_PASS_KERNELS: each pass in turn through the single-pass path's
+// kernels -- orbit table, lifetime walk and FP64 re-trace (split), or the FP64
+// lifetime kernel, then stages (b)+(c) for the pass's distinct relaxation
+// times -- into the pass's metrics slot and sigma slot.
+cudaError_t record_pass_kernels(es_batch* b)
+{
+    const es::BatchInstanceD* hi = reinterpret_cast<const es::BatchInstanceD*>(b->h_table + b->inst_offset);
+    cudaError_t e = cudaSuccess;
+    for (size_t pos = 0; e == cudaSuccess && pos < b->inst.size(); pos++) {
+        const es::BatchInstanceD& d = hi[pos];
+        const int k = b->order[pos];
+        const es_batch_grid& g = b->grids[(size_t)b->inst[(size_t)k].grid];
+        es::LifetimeLaunch L = d.L;
+        L.out = b->d_lt;
+        L.out32 = nullptr;
+        L.metrics = d.metrics;
+        L.row0 = 0;
+        L.variant = es::kLifetimePerThreadDefer;
+        L.retrace = reinterpret_cast<long long*>(b->d_retrace);
+        L.retrace_count = b->d_retrace_count;
+        L.retrace_cap = b->retrace_cap;
+        L.orbit_table = b->d_otab;
+        if (b->tuning.precision == ES_PRECISION_SPLIT)
+            e = es::launch_lifetimes_split(
+                L, es::host::long_walks(g.n_indexed, g.is.cells_per_row, g.is.cell_size, g.is.impurity_radius),
+                b->stream);
+        else
+            e = es::launch_lifetimes_fp64(L, b->stream);
+        if (e != cudaSuccess) break;
+        es::IntegrateLaunch I{};
+        I.lifetimes = b->d_lt;
+        I.phase = d.phase_sigma;
+        for (int u = 0; u < d.n_tau; u++) {
+            I.tau[u] = d.tau[u];
+            I.max_lt[u] = d.max_lt[u];
+            I.inv_tau[u] = d.inv_tau[u];
+            I.factor[u] = b->factor[(size_t)k][(size_t)u];
+        }
+        I.partial = b->d_partial;
+        I.sigma_out = b->d_psigma + pos * 2 * es::kBatchMaxTau;
+        I.w_signed = d.w_signed;
+        I.phi_integrand_factor = b->pass_phi_factor[pos];
+        I.dim = L.dim;
+        I.n_phase = L.n_phase;
+        I.n_t = d.n_tau;
+        I.n_blocks = es::kIntegrateBlocks;
+        I.fp32 = b->tuning.precision == ES_PRECISION_SPLIT ? 1 : 0;
+        e = es::launch_integrate(I, b->stream);
+    }
+    return e;
+}
+
 // Records the run sequence on the batch stream: table upload, clears, the
 // pass kernels, the FP64 re-trace, readbacks.
 es_status capture(es_batch* b)
 {
     drop_graph(b);
+    es_status st = ES_OK;
+    if (b->tuning.mode == ES_BATCH_PASS_KERNELS && (st = ensure_pass_scratch(b)) != ES_OK) return st;
     const int64_t cap = b->cap;
     es::BatchLaunch L{};
     L.inst = reinterpret_cast<const es::BatchInstanceD*>(b->d_table + b->inst_offset);
@@ -811,10 +923,15 @@ es_status capture(es_batch* b)
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_error, 0, sizeof(int), b->stream);
     if (e == cudaSuccess) {
         if (b->tuning.mode == ES_BATCH_PASS_NODES) e = record_pass_nodes(b, L);
+        else if (b->tuning.mode == ES_BATCH_PASS_KERNELS) e = record_pass_kernels(b);
         else e = es::launch_batch(L, b->tuning.precision, b->tuning.blocks_per_sm, b->tuning.mode, b->n_sm,
                                   b->total_items, b->stream);
     }
-    if (e == cudaSuccess && b->tuning.precision == ES_PRECISION_SPLIT) e = es::launch_retrace(L, b->n_sm, b->stream);
+    if (e == cudaSuccess && b->tuning.precision == ES_PRECISION_SPLIT && b->tuning.mode != ES_BATCH_PASS_KERNELS)
+        e = es::launch_retrace(L, b->n_sm, b->stream);
+    if (e == cudaSuccess && b->tuning.mode == ES_BATCH_PASS_KERNELS)
+        e = cudaMemcpyAsync(b->h_psigma, b->d_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap,
+                            cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_acc, b->d_acc, acc_bytes, cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_metrics, b->d_metrics, met_bytes, cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_error, b->d_error, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
@@ -916,6 +1033,7 @@ es_status es_batch_destroy(es_batch* b)
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graph(b);
     free_tables(b);
+    free_pass_scratch(b);
     free_grids(b);
     cudaFree(b->d_counter);
     cudaFree(b->d_error);
@@ -951,7 +1069,8 @@ es_status es_batch_set_tuning(es_batch* b, const es_batch_tuning* t)
         return bfail(b, ES_ERR_BAD_ARG, "blocks_per_sm must be 3 or 4 (got %d)", t->blocks_per_sm);
     if (t->precision != ES_PRECISION_FP64 && t->precision != ES_PRECISION_SPLIT)
         return bfail(b, ES_ERR_BAD_ARG, "unknown precision %d", t->precision);
-    if (t->mode != ES_BATCH_PASS_NODES && t->mode != ES_BATCH_GRID && t->mode != ES_BATCH_PERSISTENT)
+    if (t->mode != ES_BATCH_PASS_NODES && t->mode != ES_BATCH_GRID && t->mode != ES_BATCH_PERSISTENT &&
+        t->mode != ES_BATCH_PASS_KERNELS)
         return bfail(b, ES_ERR_BAD_ARG, "unknown batch mode %d", t->mode);
     auto item_orbits = [](const es_batch_tuning& x) {
         return x.mode == ES_BATCH_PERSISTENT ? 32LL * x.chunk_iters : 32LL * es::kBatchWarps;
@@ -1162,6 +1281,7 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
     es::BatchInstanceD* hi = reinterpret_cast<es::BatchInstanceD*>(b->h_table + b->inst_offset);
     b->factor.assign((size_t)n, {});
     b->fx_scale.assign((size_t)n, 0.0);
+    b->pass_phi_factor.assign((size_t)n, 0.0);
     long long items = 0;
     int64_t total = 0;
     for (int32_t pos = 0; pos < n; pos++) {
@@ -1223,6 +1343,7 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
         total += L.n_orbits;
         b->factor[(size_t)k] = fac;
         b->fx_scale[(size_t)k] = d.fx_scale;
+        b->pass_phi_factor[(size_t)pos] = p.phi_integrand_factor;
     }
     hdr[0] = n;
     hdr[1 + n] = items;
@@ -1233,7 +1354,7 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
     b->total_items = items;
     b->has_instances = true;
     // pass records are kernel parameters in this mode: record the graph again
-    if (b->tuning.mode == ES_BATCH_PASS_NODES) b->graph_dirty = true;
+    if (b->tuning.mode == ES_BATCH_PASS_NODES || b->tuning.mode == ES_BATCH_PASS_KERNELS) b->graph_dirty = true;
     // Re-traced orbits are a small fraction (observed ~0.05%); the list starts
     // at 1/1024 of the run and grows on overflow (es_batch_collect re-runs).
     if (b->tuning.precision == ES_PRECISION_SPLIT)
@@ -1265,7 +1386,10 @@ es_status es_batch_collect(es_batch* b, double* out_sigma, es_metrics* out_metri
     ES_BCUDA(cudaStreamSynchronize(b->stream), "batch synchronize");
     if (*b->h_error & es::kErrRetraceOverflow) {
         // the list was too short for this run: grow it to fit and run again
-        const long long need = (long long)*b->h_retrace_count;
+        // (in ES_BATCH_PASS_KERNELS the count read back is the last pass's only)
+        const long long need = b->tuning.mode == ES_BATCH_PASS_KERNELS
+                                   ? std::max((long long)*b->h_retrace_count, 2 * b->retrace_cap)
+                                   : (long long)*b->h_retrace_count;
         if ((st = ensure_retrace(b, need + need / 4 + 1024)) != ES_OK) return st;
         b->retrace_regrows++;
         if ((st = es_batch_enqueue(b)) != ES_OK) return st;
@@ -1285,11 +1409,16 @@ es_status es_batch_collect(es_batch* b, double* out_sigma, es_metrics* out_metri
         if (out_sigma) {
             double* o = out_sigma + (size_t)k * ES_BATCH_MAX_T * 2;
             for (int t = 0; t < ES_BATCH_MAX_T * 2; t++) o[t] = 0.0;
+            const double* ps = b->h_psigma + (size_t)pos * 2 * es::kBatchMaxTau;
             for (int t = 0; t < x.n_t; t++) {
                 const int u = b->t_slot[(size_t)k][(size_t)t];
                 for (int c = 0; c < 2; c++) {
-                    const long long q = (long long)acc[2 * u + c];
-                    o[2 * t + c] = ((double)q / b->fx_scale[(size_t)k]) * b->factor[(size_t)k][(size_t)u];
+                    if (b->tuning.mode == ES_BATCH_PASS_KERNELS) {
+                        o[2 * t + c] = ps[2 * u + c];
+                    } else {
+                        const long long q = (long long)acc[2 * u + c];
+                        o[2 * t + c] = ((double)q / b->fx_scale[(size_t)k]) * b->factor[(size_t)k][(size_t)u];
+                    }
                 }
             }
         }

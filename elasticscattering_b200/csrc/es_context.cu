@@ -175,17 +175,9 @@ es_status enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
     const es::LifetimeLaunch L =
         make_launch(ctx, magnetic_field, ctx->settings.particle_speed, ctx->settings.is_clockwise ? 1 : 0, ctx->coherent);
     if (ctx->desc.precision == ES_PRECISION_SPLIT) {
-        // Straight-line mean free path through the grid's disks, in cells:
-        // L / (disks filed per cell x 2 r_i). Around one cell or more (config 1:
-        // 0.87) walks end after differing numbers of cell steps and the
-        // warp-synced winner recompute pays (3% per pass on B200); well below
-        // (config 3: ~0.2) nearly every walk ends in its first cell and the
-        // synced form measured 30% slower.
-        const double cells = (double)ctx->is.cells_per_row * (double)ctx->is.cells_per_row;
-        const double per_cell = cells > 0.0 ? (double)ctx->n_imps / cells : 0.0;
-        const double mfp_cells =
-            per_cell > 0.0 ? ctx->is.cell_size / (per_cell * 2.0 * ctx->is.impurity_radius) : 1e300;
-        ES_CUDA(es::launch_lifetimes_split(L, mfp_cells >= 0.5, ctx->stream), "split lifetime kernel launch");
+        const bool defer = es::host::long_walks(ctx->n_imps, ctx->is.cells_per_row, ctx->is.cell_size,
+                                                ctx->is.impurity_radius);
+        ES_CUDA(es::launch_lifetimes_split(L, defer, ctx->stream), "split lifetime kernel launch");
         ctx->launches += 3;  // orbit table, lifetime walk, FP64 re-trace
     } else {
         ES_CUDA(es::launch_lifetimes_fp64(L, ctx->stream), "lifetime kernel launch");

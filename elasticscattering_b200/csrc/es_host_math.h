@@ -57,6 +57,20 @@ inline double integrand_factor(double particle_speed, int positions_per_row, dou
 
 // Upper bound on the cell steps of one orbit: a full circle crosses at most
 // 4 * ceil(2 pi r / cell) + a few cell edges. Exceeding it is reported.
+// Whether a grid's walks are long enough for the split lifetime kernel's
+// warp-synced winner recompute: the straight-line mean free path through its
+// disks, L / (disks filed per cell x 2 r_i), at least half a cell. Around one
+// cell or more (config 1: 0.87) walks end after differing numbers of cell
+// steps and the synced form pays (3% per pass on B200); well below (config 3:
+// ~0.2) nearly every walk ends in its first cell and it measured 30% slower.
+inline bool long_walks(int64_t n_indexed, int cells_per_row, double cell_size, double impurity_radius)
+{
+    const double cells = (double)cells_per_row * (double)cells_per_row;
+    const double per_cell = cells > 0.0 ? (double)n_indexed / cells : 0.0;
+    if (!(per_cell > 0.0) || !(impurity_radius > 0.0)) return true;
+    return cell_size / (per_cell * 2.0 * impurity_radius) >= 0.5;
+}
+
 inline int walk_cap_for(double radius, double cell)
 {
     const double steps = 4.0 * std::ceil(kPI2 * radius / cell) + 16.0;

@@ -33,6 +33,8 @@ def main() -> None:
     ap.add_argument("--compare-split", action="store_true", help="time plain FP64 against split precision")
     ap.add_argument("--batch", action="store_true",
                     help="run the pass through the batched kernel (one instance, fused integration)")
+    ap.add_argument("--mode", type=int, default=N.ES_BATCH_PERSISTENT,
+                    help="--batch: es_batch_mode (0 pass nodes, 1 grid, 2 persistent, 3 single-pass kernels)")
     ap.add_argument("--chunk-iters", type=int, default=32)
     ap.add_argument("--sweep-sample", type=int, default=None,
                     help="--batch: run sample K of the 64-sample batched sweep draw instead of --workload")
@@ -96,7 +98,7 @@ def batch_pass(a) -> None:
     s = make_settings(w.tau, w.alpha, w.clockwise, w.particle_speed, w.region_size, w.region_extends, w.density,
                       w.impurity_radius, w.target_cell_population)
     prec = N.ES_PRECISION_SPLIT if a.precision is None else a.precision
-    with BatchSweep(chunk_iters=a.chunk_iters, precision=prec) as b:
+    with BatchSweep(chunk_iters=a.chunk_iters, precision=prec, mode=a.mode) as b:
         gid = b.add_grid(g)
         b.set_passes([BatchPass(gid, w.dim, w.phi_steps, bool(a.coherent), w.region_size, g.info().cell_size,
                                 a.field, s, list(w.temperatures))])
@@ -126,7 +128,7 @@ def batch_sweep_sample(a) -> None:
     smp = wl.samples[a.sweep_sample]
     g = Grid.from_seed(smp.seed, wl.region_size, wl.region_extends, smp.density, wl.impurity_radius, a.tcp)
     prec = N.ES_PRECISION_SPLIT if a.precision is None else a.precision
-    with BatchSweep(chunk_iters=a.chunk_iters, precision=prec) as b:
+    with BatchSweep(chunk_iters=a.chunk_iters, precision=prec, mode=a.mode) as b:
         gid = b.add_grid(g)
         b.set_passes(sweep_passes(wl, {smp.index: gid}, {smp.index: g.info().cell_size}, samples=[smp]))
         ms = []

@@ -277,8 +277,12 @@ typedef enum es_batch_mode {
                                  as kernel parameter; one block per 256 orbits */
     ES_BATCH_GRID = 1,        /* one kernel over all passes, one block per 256 orbits, each block looks
                                  its pass up in the device table */
-    ES_BATCH_PERSISTENT = 2   /* one persistent kernel: warps take work items of 32 * chunk_iters
+    ES_BATCH_PERSISTENT = 2,  /* one persistent kernel: warps take work items of 32 * chunk_iters
                                  orbits of any pass from a global counter */
+    ES_BATCH_PASS_KERNELS = 3 /* the single-pass path's kernels for each pass in turn: the lifetime
+                                 kernel (and, split, its FP64 re-trace) writes the pass's lifetimes
+                                 to device scratch, the integration kernels reduce them to sigma;
+                                 chunk_iters and blocks_per_sm are not used */
 } es_batch_mode;
 
 /* Launch choices of a batch (picked by the autotuner). */

@@ -92,8 +92,8 @@ def reference(sweep_inputs, cuda_device):
     return per_pass_reference(grids, passes, cuda_device)
 
 
-def new_batch(grids, device, precision, chunk_iters=8, blocks_per_sm=4):
-    b = BatchSweep(device, chunk_iters=chunk_iters, blocks_per_sm=blocks_per_sm, precision=precision)
+def new_batch(grids, device, precision, chunk_iters=8, blocks_per_sm=4, mode=N.ES_BATCH_PERSISTENT):
+    b = BatchSweep(device, chunk_iters=chunk_iters, blocks_per_sm=blocks_per_sm, precision=precision, mode=mode)
     ids = {k: b.add_grid(grids[k]) for k, *_rest in SAMPLES}
     return b, ids
 
@@ -232,3 +232,29 @@ def test_autotuner_picks_from_measured_candidates_and_caches(tmp_path, cuda_devi
     again = autotune.tune_sweep(wl, device=cuda_device, n_classes=2, cache=cache, tcp_candidates=(6, 16),
                                 shape_candidates=shapes)
     assert again == r
+
+
+@pytest.mark.parametrize("precision,rtol", [(N.ES_PRECISION_FP64, FP64_RTOL), (N.ES_PRECISION_SPLIT, SPLIT_RTOL)])
+def test_batch_pass_kernels_mode(sweep_inputs, reference, cuda_device, precision, rtol):
+    """ES_BATCH_PASS_KERNELS runs the single-pass path's kernels for each pass
+    (lifetimes to device scratch, then the integration kernels): the same sigma
+    as the per-pass FP64 path within the precision's bar, the same counters, and
+    the same bits on a second replay."""
+    ext, grids = sweep_inputs
+    ref_sigma, ref_mets = reference
+    b, ids = new_batch(grids, cuda_device, precision)
+    try:
+        b.set_tuning(mode=N.ES_BATCH_PASS_KERNELS)
+        b.set_passes(make_passes(ext, grids, ids))
+        out, mets = b.run()
+        again, mets2 = b.run()
+        got = out[:, :len(TEMPS), :]
+        err = rel_err(got, ref_sigma)
+        assert float(err.max()) <= rtol, (precision, float(err.max()), np.unravel_index(err.argmax(), err.shape))
+        for n, (m, r) in enumerate(zip(mets, ref_mets)):
+            for k in METRIC_KEYS:
+                assert m[k] == r[k], (precision, n, k, m[k], r[k])
+        assert np.array_equal(out.view(np.int64), again.view(np.int64)) and mets == mets2
+        assert out[:, len(TEMPS):, :].max() == 0.0 and out[:, len(TEMPS):, :].min() == 0.0
+    finally:
+        b.close()
