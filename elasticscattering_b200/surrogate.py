@@ -205,7 +205,9 @@ class Simulator:
         self.device = device
         self.levels = np.exp(np.linspace(math.log(N_RANGE[0]), math.log(N_RANGE[1]), self.res.density_levels))
         self.grids = {}
-        self.batch = BatchSweep(device)
+        # thousands of small passes per call: the one persistent kernel, which
+        # has no per-pass launches (the per-pass-kernels default suits large passes)
+        self.batch = BatchSweep(device, mode=N.ES_BATCH_PERSISTENT)
         self.grid_ids = {}
 
     def close(self) -> None:
