@@ -33,6 +33,30 @@ def test_library_exports_every_declared_symbol(header, loader):
     assert not missing, missing
 
 
+def test_python_constants_match_header_enums():
+    """Every ES_* enumerator and #define of include/es_cuda.h that the Python
+    binding names has the header's value (batch modes, precisions, status codes)."""
+    text = (ROOT / "include" / "es_cuda.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    values = {}
+    for body in re.findall(r"enum\s+\w*\s*\{(.*?)\}", text, flags=re.S):
+        nxt = 0
+        for item in body.split(","):
+            item = item.strip()
+            if not item:
+                continue
+            name, _, val = item.partition("=")
+            nxt = int(val.strip(), 0) if val.strip() else nxt
+            values[name.strip()] = nxt
+            nxt += 1
+    for name, val in re.findall(r"#define\s+(ES_[A-Z0-9_]+)\s+(-?\d+)", text):
+        values[name] = int(val)
+    checked = [n for n in values if hasattr(_native, n)]
+    assert {"ES_BATCH_PASS_KERNELS", "ES_BATCH_PERSISTENT", "ES_PRECISION_SPLIT", "ES_OK"} <= set(checked)
+    for n in checked:
+        assert getattr(_native, n) == values[n], (n, getattr(_native, n), values[n])
+
+
 def test_python_binding_declares_every_symbol():
     for header, api in (("es_cuda.h", _native.CUDA_API), ("es_host.h", _native.HOST_API)):
         assert set(declared_symbols(header)) == set(api), header
