@@ -936,7 +936,7 @@ def profiled_issue(name: str):
     if len(out) != 2:
         return None
     out["lane_frac"] = out["threads_per_instruction"] / 32.0
-    out["source"] = f"ncu --set full summary, profiles/{p.name} (config-1 pass, B = 20 T)"
+    out["source"] = f"ncu --set full summary, profiles/{p.name} (one 257^2 x 516-orbit pass, B = 20 T)"
     return out
 
 

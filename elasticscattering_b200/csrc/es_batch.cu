@@ -635,8 +635,8 @@ struct es_batch {
     cudaStream_t stream = nullptr;
     char err[512] = "";
     int64_t launches = 0;
-    // measured best on B200 for config-1- and config-2-sized passes (12-16% ahead of
-    // ES_BATCH_PERSISTENT on 129^2 to 513^2 start grids; the autotuner may choose otherwise)
+    // measured best on B200 for passes of 129^2 to 513^2 start positions x 516 phases
+    // (12-16% ahead of ES_BATCH_PERSISTENT; the autotuner may choose otherwise)
     es_batch_tuning tuning{32, 4, ES_PRECISION_SPLIT, ES_BATCH_PASS_KERNELS};
     int64_t captured_items = -1;              // grid size recorded in the graph (ES_BATCH_GRID)
     static constexpr int kBranches = 8;       // parallel graph branches (ES_BATCH_PASS_NODES)

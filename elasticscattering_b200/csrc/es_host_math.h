@@ -60,9 +60,10 @@ inline double integrand_factor(double particle_speed, int positions_per_row, dou
 // Whether a grid's walks are long enough for the split lifetime kernel's
 // warp-synced winner recompute: the straight-line mean free path through its
 // disks, L / (disks filed per cell x 2 r_i), at least half a cell. Around one
-// cell or more (config 1: 0.87) walks end after differing numbers of cell
-// steps and the synced form pays (3% per pass on B200); well below (config 3:
-// ~0.2) nearly every walk ends in its first cell and it measured 30% slower.
+// cell or more (5e15 m^-2, r_i 2 nm, 49 nm cells: 0.87) walks end after
+// differing numbers of cell steps and the synced form pays (3% per pass on
+// B200); well below (1e16 m^-2, r_i 5 nm, 35 nm cells: ~0.2) nearly every walk
+// ends in its first cell and it measured 30% slower.
 inline bool long_walks(int64_t n_indexed, int cells_per_row, double cell_size, double impurity_radius)
 {
     const double cells = (double)cells_per_row * (double)cells_per_row;

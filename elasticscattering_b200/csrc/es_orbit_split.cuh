@@ -464,7 +464,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
             // its annulus, with few lanes active. Pass 1 only marks each lane's
             // candidates in a bit mask, and pass 2 runs the test per candidate in
             // disk order, so the warp runs it as often as its busiest lane has
-            // candidates: 1.5% (B = 20 T) to 4% (B = 1 T; config 3) faster per
+            // candidates: 1.5% (B = 20 T) to 4% (B = 1 T; 1e16 m^-2) faster per
             // pass on B200. The batched kernel keeps one loop (1.3% slower there).
             for (int kb = k0; kb < k1; kb += 32) {
                 const int kn = min(32, k1 - kb);
@@ -701,9 +701,9 @@ __device__ __forceinline__ bool split_orbit(const F& f, long long g, SplitCounte
 // their walks after different numbers of cell steps; they meet at a __syncwarp
 // before the FP64 winner recompute, so that code (sqrt, asin and divisions of
 // the reference's GetCrossPoints/GetAngle) runs once per warp instead of once
-// per distinct exit step: 3% faster per config-1 pass on B200 in the
-// single-pass kernel. Every lane reaches the sync: the walk is bounded by the
-// walk cap and every path returns. The batched kernels keep split_orbit (the
+// per distinct exit step: 3% faster on B200 per single-pass launch of 257^2 x
+// 516 orbits at 5e15 m^-2. Every lane reaches the sync: the walk is bounded by
+// the walk cap and every path returns. The batched kernels keep split_orbit (the
 // deferred form measured 7% slower there, where the orbit's integrand follows
 // the walk in the same kernel).
 template <class F>
