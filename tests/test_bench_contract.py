@@ -27,3 +27,21 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["config"]["workload"].startswith("config0")
+
+
+def test_roofline_figures_come_from_the_committed_profiles():
+    """The GPU arm's `roofline.traffic` and `roofline.issue` are read from the
+    committed ncu summaries: every lifetime-kernel summary carries the
+    machine-readable lines, and the traffic scales with the orbits per launch."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    for name in ("split", "fp64"):
+        issue = bench.profiled_issue(name)
+        assert issue is not None, name
+        assert 0.0 < issue["issue_active_frac"] <= 1.0 and 0.0 < issue["threads_per_instruction"] <= 32.0
+        assert abs(issue["lane_frac"] - issue["threads_per_instruction"] / 32.0) < 1e-12
+        t1 = bench.profiled_traffic(name)
+        assert t1 and t1 > 8 * 34_081_284  # at least the FP64 lifetime write of a 257^2 x 516 pass
+    full = bench.profiled_traffic("split", 34_081_284)
+    half = bench.profiled_traffic("split", 34_081_284 // 2)
+    assert abs(full - 2 * half) / full < 1e-6
