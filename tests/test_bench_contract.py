@@ -41,7 +41,9 @@ def test_roofline_figures_come_from_the_committed_profiles():
         assert 0.0 < issue["issue_active_frac"] <= 1.0 and 0.0 < issue["threads_per_instruction"] <= 32.0
         assert abs(issue["lane_frac"] - issue["threads_per_instruction"] / 32.0) < 1e-12
         t1 = bench.profiled_traffic(name)
-        assert t1 and t1 > 8 * 34_081_284  # at least the FP64 lifetime write of a 257^2 x 516 pass
+        # most of the 8-byte lifetime write of a 257^2 x 516 pass (part of it can
+        # still sit in the 126 MB L2 when the kernel ends)
+        assert t1 and t1 > 0.5 * 8 * 34_081_284
     full = bench.profiled_traffic("split", 34_081_284)
     half = bench.profiled_traffic("split", 34_081_284 // 2)
     assert abs(full - 2 * half) / full < 1e-6
