@@ -13,6 +13,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 
 ES_OK = 0
+ES_ERR_BAD_ARG = 1
 STATUS_NAMES = {
     0: "ES_OK", 1: "ES_ERR_BAD_ARG", 2: "ES_ERR_OOM", 3: "ES_ERR_LAUNCH", 4: "ES_ERR_WALK_CAP",
     5: "ES_ERR_DEVICE", 6: "ES_ERR_NO_GRID", 7: "ES_ERR_NO_SAMPLE", 8: "ES_ERR_TIMEOUT",
@@ -101,6 +102,9 @@ CUDA_API = {
     "es_compute_sigmas_images": (_i32, [_vp, _d, _vp, _i32, _vp, _vp, _vp, _vp, C.POINTER(Metrics)]),
     "es_compute_lifetimes": (_i32, [_vp, _d, _vp, C.POINTER(Metrics)]),
     "es_derive_temperatures": (_i32, [_vp, _vp, _i32, _vp]),
+    "es_read_lifetimes": (_i32, [_vp, _i64, _i64, _vp]),
+    "es_set_rows": (_i32, [_vp, _i32, _i32]),
+    "es_enqueue_derive_temperatures": (_i32, [_vp, _vp, _i32, _vp]),
     "es_enqueue_sigmas": (_i32, [_vp, _d, _vp, _i32, _vp]),
     "es_enqueue_lifetimes": (_i32, [_vp, _d]),
     "es_synchronize": (_i32, [_vp]),

@@ -169,3 +169,69 @@ class BatchSweep:
 
     def launch_count(self) -> int:
         return int(N.cuda_lib().es_batch_launch_count(self._b))
+
+
+def finish_results(coherent: np.ndarray, incoherent: np.ndarray) -> dict:
+    """SimulationRunner::FinishResults (src/SimulationRunner.cpp:153-198) on the
+    per-sample sigmas of a sweep: `coherent` and `incoherent` are
+    [sample][field][temperature][xx, xy]. Returns the sample means of each sector
+    and delta_xx = std(sigma_xx_coh + sigma_xx_inc) / mean per (field,
+    temperature), summed over the samples in sample order as the reference does,
+    so the result does not depend on which GPU computed which sample."""
+    coh = np.asarray(coherent, dtype=np.float64)
+    inc = np.asarray(incoherent, dtype=np.float64)
+    S = coh.shape[0]
+    c_sum = np.zeros(coh.shape[1:])
+    i_sum = np.zeros(inc.shape[1:])
+    dxx_sq = np.zeros(coh.shape[1:3])
+    for s in range(S):
+        c_sum = c_sum + coh[s]
+        i_sum = i_sum + inc[s]
+        t = coh[s, :, :, 0] + inc[s, :, :, 0]
+        dxx_sq = dxx_sq + t * t
+    c_mean = c_sum / float(S)
+    i_mean = i_sum / float(S)
+    if S == 1:
+        xxd = np.zeros(coh.shape[1:3])
+    else:
+        sq_exp = dxx_sq / float(S)
+        exp = c_mean[:, :, 0] + i_mean[:, :, 0]
+        xxd = np.sqrt((sq_exp - exp * exp) / (float(S) - 1.0)) / exp
+    return {"coherent": c_mean, "incoherent": i_mean, "delta_xx": xxd}
+
+
+def gather_sweep(local: dict, n_samples: int, dist=None) -> tuple:
+    """The one exchange of a multi-GPU sweep: every rank holds the sigmas of its
+    own samples, {sample index: (coherent [field][T][2], incoherent [field][T][2])};
+    all of them are gathered (torch.distributed all_gather_object, any backend)
+    and returned as dense [sample][field][T][2] arrays in sample order. With
+    dist None (one process) the local results are returned as they are."""
+    parts = [local]
+    if dist is not None and dist.is_initialized() and dist.get_world_size() > 1:
+        parts = [None] * dist.get_world_size()
+        dist.all_gather_object(parts, local)
+    merged = {}
+    for p in parts:
+        for k, v in p.items():
+            if k in merged:
+                raise ValueError(f"sample {k} was computed by more than one rank")
+            merged[k] = v
+    if sorted(merged) != list(range(n_samples)):
+        raise ValueError(f"gathered samples {sorted(merged)} are not 0..{n_samples - 1}")
+    coh = np.stack([np.asarray(merged[k][0], dtype=np.float64) for k in range(n_samples)])
+    inc = np.stack([np.asarray(merged[k][1], dtype=np.float64) for k in range(n_samples)])
+    return coh, inc
+
+
+def per_sample_sigmas(passes: list, out: np.ndarray, sample_of_grid: dict, n_fields: int, n_t: int) -> dict:
+    """Regroups a batch's results ([pass][T][2], passes as sweep_passes orders
+    them: per sample, per field, coherent then incoherent) into
+    {sample index: (coherent [field][T][2], incoherent [field][T][2])}."""
+    res = {}
+    for k, p in enumerate(passes):
+        s = sample_of_grid[p.grid]
+        if s not in res:
+            res[s] = (np.zeros((n_fields, n_t, 2)), np.zeros((n_fields, n_t, 2)))
+        f = (k // 2) % n_fields
+        res[s][0 if p.coherent else 1][f] = out[k, :n_t, :]
+    return res

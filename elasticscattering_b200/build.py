@@ -5,8 +5,9 @@
                     SimulationCUDA) over the C ABI
     es_b200         the command-line driver (drop-in for the reference's CLI)
 
-Plain nvcc/g++ invocations, rebuilt only when a source is newer than its
-output. Used by __graft_entry__.build() and by `python -m elasticscattering_b200.build`.
+Plain nvcc/g++ invocations, rebuilt when a source is newer than its output,
+or always with force=True (what __graft_entry__.build() asks for). Used by
+__graft_entry__.build() and by `python -m elasticscattering_b200.build`.
 """
 from __future__ import annotations
 
@@ -78,7 +79,7 @@ def _headers(d: Path) -> list[Path]:
     return sorted(list(d.glob("*.h")) + list(d.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
 
 
-def build_cuda(verbose_ptxas: bool = False) -> Path:
+def build_cuda(verbose_ptxas: bool = False, force: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
     out = PKG / "libes_cuda.so"
     hdrs = _headers(CSRC)
@@ -88,19 +89,19 @@ def build_cuda(verbose_ptxas: bool = False) -> Path:
         src = CSRC / unit
         obj = OBJ / (unit + ".o")
         objs.append(obj)
-        if verbose_ptxas or _stale(obj, [src] + hdrs):
+        if force or verbose_ptxas or _stale(obj, [src] + hdrs):
             cmd = [nvcc()] + NVCC_COMMON + flags + ["-c", str(src), "-o", str(obj)]
             if verbose_ptxas:
                 cmd += ["-Xptxas", "-v"]
             jobs.append(cmd)
     with ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
         list(ex.map(_run, jobs))
-    if jobs or _stale(out, objs):
+    if force or jobs or _stale(out, objs):
         _run([nvcc()] + ARCH + ["-shared", "-o", str(out)] + [str(o) for o in objs])
     return out
 
 
-def build_host() -> list[Path]:
+def build_host(force: bool = False) -> list[Path]:
     """Host C++ runtime: libes_host.so (+ the es_b200 CLI once main.cpp exists)."""
     srcs = [HOST / u for u in HOST_UNITS if (HOST / u).exists()]
     if not srcs:
@@ -108,14 +109,14 @@ def build_host() -> list[Path]:
     OBJ.mkdir(exist_ok=True)
     lib = PKG / "libes_host.so"
     hdrs = _headers(HOST)
-    if _stale(lib, srcs + hdrs + [PKG / "libes_cuda.so"]):
+    if force or _stale(lib, srcs + hdrs + [PKG / "libes_cuda.so"]):
         _run(["g++"] + GXX_COMMON + ["-shared", "-o", str(lib)] + [str(s) for s in srcs]
              + [f"-L{PKG}", "-les_cuda", "-Wl,-rpath,$ORIGIN"])
     out = [lib]
     main = HOST / "main.cpp"
     cli = PKG / "es_b200"
     if main.exists():
-        if _stale(cli, [main, lib] + hdrs):
+        if force or _stale(cli, [main, lib] + hdrs):
             _run(["g++"] + GXX_COMMON + ["-o", str(cli), str(main), f"-L{PKG}", "-les_host", "-les_cuda",
                                           "-Wl,-rpath,$ORIGIN"])
         out.append(cli)
@@ -127,9 +128,10 @@ def build_oracle() -> None:
     _run(["make", "-s", "-C", str(ROOT / "oracle")])
 
 
-def build_all(verbose_ptxas: bool = False) -> None:
-    build_cuda(verbose_ptxas)
-    build_host()
+def build_all(verbose_ptxas: bool = False, force: bool = False) -> None:
+    """force: recompile every unit whatever the timestamps (the build check)."""
+    build_cuda(verbose_ptxas, force)
+    build_host(force)
     build_oracle()
 
 

@@ -74,6 +74,7 @@ struct es_ctx {
     long long retrace_cap = 0;
     es_tuning tuning{es::kLifetimePerThreadDefer};
     bool lifetimes_valid = false;
+    int row0 = 0, row1 = 0;  // start rows [row0, row1) of the passes (es_set_rows); row1 = dim by default
 };
 
 namespace {
@@ -149,14 +150,14 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.dist = ctx->desc.region_size / (double)(ctx->desc.positions_per_row - 1);
     L.off_x = ctx->desc.grid_cell_size * 0.01;
     L.off_y = ctx->desc.grid_cell_size * 0.005;
-    L.n_orbits = ctx->n_orbits;
+    L.n_orbits = (int64_t)(ctx->row1 - ctx->row0) * ctx->desc.positions_per_row * ctx->n_phase;
     L.cpr = ctx->is.cells_per_row;
     L.dim = ctx->desc.positions_per_row;
     L.n_phase = ctx->n_phase;
     L.clockwise = clockwise;
     L.coherent = coherent;
     L.walk_cap = es::host::walk_cap_for(L.radius, L.cell_size);
-    L.row0 = 0;
+    L.row0 = ctx->row0;
     L.variant = ctx->tuning.lifetime_variant;
     L.work = ctx->d_work;
     L.imps32 = ctx->d_imps32;
@@ -188,10 +189,27 @@ es_status enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
     return ES_OK;
 }
 
+// Every temperature of a call is checked before its first launch, so an
+// ES_ERR_BAD_ARG return means nothing of the call was enqueued.
+es_status check_temperatures(es_ctx* ctx, const double* temperatures, int32_t n_t)
+{
+    if (n_t < 0 || (n_t > 0 && !temperatures)) return fail(ctx, ES_ERR_BAD_ARG, "bad temperature list");
+    for (int32_t k = 0; k < n_t; k++) {
+        const double T = temperatures[k];
+        if (!ctx->coherent && !(T > 0.0))
+            return fail(ctx, ES_ERR_BAD_ARG, "temperature %g: the incoherent sector needs T > 0", T);
+        if (!std::isfinite(T) && !ctx->coherent)
+            return fail(ctx, ES_ERR_BAD_ARG, "temperature %g is not finite", T);
+    }
+    return ES_OK;
+}
+
 // Stages (b)+(c) for all temperatures on the resident lifetimes; results to a
 // device array of 2*n_t doubles. pos != nullptr also writes the image maps.
 es_status enqueue_integrate(es_ctx* ctx, const double* temperatures, int32_t n_t, double* d_out, double* pos)
 {
+    es_status st = check_temperatures(ctx, temperatures, n_t);
+    if (st != ES_OK) return st;
     const double w = ctx->last_w;
     const double w_signed = ctx->settings.is_clockwise ? -w : w;  // SimulationCPU.cpp:108
     for (int32_t t0 = 0; t0 < n_t; t0 += es::kMaxTChunk) {
@@ -200,10 +218,7 @@ es_status enqueue_integrate(es_ctx* ctx, const double* temperatures, int32_t n_t
         L.lifetimes = ctx->d_lifetimes;
         L.phase = ctx->d_phase_sigma;
         for (int k = 0; k < nc; k++) {
-            const double T = temperatures[t0 + k];
-            if (!ctx->coherent && !(T > 0.0))
-                return fail(ctx, ES_ERR_BAD_ARG, "temperature %g: the incoherent sector needs T > 0", T);
-            const double tau = get_tau(ctx, T);
+            const double tau = get_tau(ctx, temperatures[t0 + k]);
             L.tau[k] = tau;
             L.max_lt[k] = 15.0 * tau;  // GetDefaultMaxLifetime, Simulation.h:91
             L.inv_tau[k] = 1.0 / tau;
@@ -221,6 +236,8 @@ es_status enqueue_integrate(es_ctx* ctx, const double* temperatures, int32_t n_t
         L.dim = ctx->desc.positions_per_row;
         L.n_phase = ctx->n_phase;
         L.n_t = nc;
+        L.row0 = ctx->row0;
+        L.rows = ctx->row1 - ctx->row0;
         L.n_blocks = es::kIntegrateBlocks;
         L.fp32 = ctx->desc.precision == ES_PRECISION_SPLIT ? 1 : 0;
         ES_CUDA(es::launch_integrate(L, ctx->stream), "integration kernel launch");
@@ -347,6 +364,8 @@ es_status es_create(const es_sim_desc* desc, es_ctx** out)
     ctx->n_phase = (int)n_phase;
     ctx->n_pos = (int)n_pos;
     ctx->n_orbits = n_pos * n_phase;
+    ctx->row0 = 0;
+    ctx->row1 = desc->positions_per_row;
 
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
@@ -457,6 +476,18 @@ es_status es_set_tuning(es_ctx* ctx, const es_tuning* tuning)
     if (tuning->lifetime_variant < 0 || tuning->lifetime_variant >= es::kLifetimeVariants)
         return fail(ctx, ES_ERR_BAD_ARG, "unknown lifetime variant %d", tuning->lifetime_variant);
     ctx->tuning = *tuning;
+    return ES_OK;
+}
+
+es_status es_set_rows(es_ctx* ctx, int32_t j0, int32_t j1)
+{
+    if (!ctx) return ES_ERR_BAD_ARG;
+    if (j0 < 0 || j1 <= j0 || j1 > ctx->desc.positions_per_row)
+        return fail(ctx, ES_ERR_BAD_ARG, "es_set_rows: rows [%d, %d) outside 0..%d", j0, j1,
+                    ctx->desc.positions_per_row);
+    ctx->row0 = j0;
+    ctx->row1 = j1;
+    ctx->lifetimes_valid = false;
     return ES_OK;
 }
 
@@ -574,13 +605,29 @@ es_status es_compute_lifetimes(es_ctx* ctx, double magnetic_field, double* out_l
     return read_device_error(ctx);
 }
 
+es_status es_read_lifetimes(es_ctx* ctx, int64_t first, int64_t count, double* out)
+{
+    es_status st = bind(ctx);
+    if (st != ES_OK) return st;
+    if (!ctx->lifetimes_valid) return fail(ctx, ES_ERR_BAD_ARG, "no resident lifetimes: call es_compute_lifetimes first");
+    if (first < 0 || count < 0 || first > ctx->n_orbits || count > ctx->n_orbits - first || (count > 0 && !out))
+        return fail(ctx, ES_ERR_BAD_ARG, "es_read_lifetimes: range [%lld, +%lld) outside the %lld orbits of the pass",
+                    (long long)first, (long long)count, (long long)ctx->n_orbits);
+    if (count == 0) return ES_OK;
+    ES_CUDA(cudaMemcpyAsync(out, ctx->d_lifetimes + first, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream),
+            "lifetime readback");
+    ES_CUDA(cudaStreamSynchronize(ctx->stream), "lifetime readback");
+    return ES_OK;
+}
+
 es_status es_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_t n_t, double* out_sigma)
 {
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if ((st = check_ready(ctx)) != ES_OK) return st;
     if (!ctx->lifetimes_valid) return fail(ctx, ES_ERR_BAD_ARG, "no resident lifetimes: call es_compute_lifetimes first");
-    if (n_t < 0 || (n_t > 0 && (!temperatures || !out_sigma))) return fail(ctx, ES_ERR_BAD_ARG, "bad temperature list");
+    if (n_t > 0 && !out_sigma) return fail(ctx, ES_ERR_BAD_ARG, "bad temperature list");
+    if ((st = check_temperatures(ctx, temperatures, n_t)) != ES_OK) return st;
     for (int32_t t0 = 0; t0 < n_t; t0 += es::kMaxTChunk) {
         const int nc = (n_t - t0) < es::kMaxTChunk ? (n_t - t0) : es::kMaxTChunk;
         if ((st = enqueue_integrate(ctx, temperatures + t0, nc, ctx->d_sigma, nullptr)) != ES_OK) return st;
@@ -595,7 +642,12 @@ es_status es_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_
 es_status es_compute_sigmas(es_ctx* ctx, double magnetic_field, const double* temperatures, int32_t n_t,
                             double* out_sigma, es_metrics* out_metrics)
 {
-    es_status st = es_compute_lifetimes(ctx, magnetic_field, nullptr, out_metrics);
+    es_status st = bind(ctx);
+    if (st != ES_OK) return st;
+    if ((st = check_ready(ctx)) != ES_OK) return st;
+    if (n_t > 0 && !out_sigma) return fail(ctx, ES_ERR_BAD_ARG, "bad temperature list");
+    if ((st = check_temperatures(ctx, temperatures, n_t)) != ES_OK) return st;
+    st = es_compute_lifetimes(ctx, magnetic_field, nullptr, out_metrics);
     if (st != ES_OK) return st;
     return es_derive_temperatures(ctx, temperatures, n_t, out_sigma);
 }
@@ -604,10 +656,16 @@ es_status es_compute_sigmas_images(es_ctx* ctx, double magnetic_field, const dou
                                    double* out_sigma, double* lifetime_pos, double* sigma_xx_pos,
                                    double* sigma_xy_pos, es_metrics* out_metrics)
 {
-    es_status st = es_compute_lifetimes(ctx, magnetic_field, nullptr, out_metrics);
+    es_status st = bind(ctx);
     if (st != ES_OK) return st;
+    if ((st = check_ready(ctx)) != ES_OK) return st;
     if (n_t < 0 || (n_t > 0 && (!temperatures || !out_sigma || !lifetime_pos || !sigma_xx_pos || !sigma_xy_pos)))
         return fail(ctx, ES_ERR_BAD_ARG, "bad image arguments");
+    if (ctx->row0 != 0 || ctx->row1 != ctx->desc.positions_per_row)
+        return fail(ctx, ES_ERR_BAD_ARG, "the per-position maps need every start row (es_set_rows)");
+    if ((st = check_temperatures(ctx, temperatures, n_t)) != ES_OK) return st;
+    st = es_compute_lifetimes(ctx, magnetic_field, nullptr, out_metrics);
+    if (st != ES_OK) return st;
     if ((st = ensure_pos(ctx, es::kMaxTChunk)) != ES_OK) return st;
     for (int32_t t0 = 0; t0 < n_t; t0 += es::kMaxTChunk) {
         const int nc = (n_t - t0) < es::kMaxTChunk ? (n_t - t0) : es::kMaxTChunk;
@@ -637,7 +695,18 @@ es_status es_enqueue_sigmas(es_ctx* ctx, double magnetic_field, const double* te
     if (st != ES_OK) return st;
     if ((st = check_ready(ctx)) != ES_OK) return st;
     if (n_t < 0 || (n_t > 0 && (!temperatures || !d_out_sigma))) return fail(ctx, ES_ERR_BAD_ARG, "bad temperature list");
+    if ((st = check_temperatures(ctx, temperatures, n_t)) != ES_OK) return st;
     if ((st = enqueue_lifetimes(ctx, magnetic_field)) != ES_OK) return st;
+    return enqueue_integrate(ctx, temperatures, n_t, d_out_sigma, nullptr);
+}
+
+es_status es_enqueue_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_t n_t, double* d_out_sigma)
+{
+    es_status st = bind(ctx);
+    if (st != ES_OK) return st;
+    if ((st = check_ready(ctx)) != ES_OK) return st;
+    if (!ctx->lifetimes_valid) return fail(ctx, ES_ERR_BAD_ARG, "no resident lifetimes: call es_compute_lifetimes first");
+    if (n_t > 0 && !d_out_sigma) return fail(ctx, ES_ERR_BAD_ARG, "bad temperature list");
     return enqueue_integrate(ctx, temperatures, n_t, d_out_sigma, nullptr);
 }
 
@@ -654,6 +723,8 @@ es_status es_average_lifetime(es_ctx* ctx, double* out_average)
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if (!out_average) return fail(ctx, ES_ERR_BAD_ARG, "es_average_lifetime: null output");
+    if (ctx->row0 != 0 || ctx->row1 != ctx->desc.positions_per_row)
+        return fail(ctx, ES_ERR_BAD_ARG, "es_average_lifetime needs every start row (es_set_rows)");
     if (!ctx->lifetimes_valid) return fail(ctx, ES_ERR_BAD_ARG, "no resident lifetimes: call es_compute_lifetimes first");
     ES_CUDA(es::launch_lifetime_sum(ctx->d_lifetimes, ctx->n_orbits, ctx->d_partial, ctx->d_sigma, ctx->stream),
             "lifetime sum");

@@ -104,8 +104,17 @@ struct IntegrateLaunch {
     double w_signed;
     double phi_integrand_factor;
     int dim, n_phase, n_t;        // n_t <= kMaxTChunk
+    int row0, rows;               // start rows [row0, row0 + rows) of the pass (rows 0: every row)
     int n_blocks;                 // partial blocks per temperature
     int fp32;                     // 1: the FP32 Boltzmann kernel of the split path (es_sigma32.cuh)
+    // Filled by launch_integrate from the fields above (FP32 split kernel):
+    // 1 / tau and w tau in FP32, and sin h, cos h (h = w 15 tau / 2) and
+    // 1 - exp(-15) of a lifetime truncated at 15 tau.
+    float inv_tau_f[kMaxTChunk];
+    float wtau_f[kMaxTChunk];
+    float trunc_sh[kMaxTChunk];
+    float trunc_ch[kMaxTChunk];
+    float trunc_e1[kMaxTChunk];
 };
 
 // Message returned by es_last_error(NULL), for entry points without a context.

@@ -34,6 +34,30 @@ __device__ __forceinline__ void sincos_reduced(double x, float& s_out, float& c_
     c_out = (n == 0) ? c : (n == 1) ? -s : (n == 2) ? -c : s;
 }
 
+// sincos_reduced with the quadrant taken by the round-to-integer constant
+// 1.5 * 2^52 instead of rint and an FP64-to-integer conversion: fma(x, 2/pi,
+// 1.5 * 2^52) holds round(x * 2/pi) in its low mantissa bits (|x| * 2/pi
+// below 2^51), read with a register move. The polynomials are sincos_reduced's.
+__device__ __forceinline__ void sincos_reduced_fast(double x, float& s_out, float& c_out)
+{
+    constexpr double kTwoOverPi = 0.636619772367581343076;
+    constexpr double kHalfPi = 1.570796326794896619231;
+    constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+    const double t = fma(x, kTwoOverPi, kRound);
+    const double q = t - kRound;
+    const float r = (float)fma(-q, kHalfPi, x);
+    const float r2 = r * r;
+    const float s =
+        fmaf(r * r2, fmaf(r2, fmaf(r2, fmaf(r2, 1.0f / 362880.0f, -1.0f / 5040.0f), 1.0f / 120.0f), -1.0f / 6.0f), r);
+    const float c = fmaf(
+        r2, fmaf(r2, fmaf(r2, fmaf(r2, fmaf(r2, -1.0f / 3628800.0f, 1.0f / 40320.0f), -1.0f / 720.0f), 1.0f / 24.0f),
+                 -0.5f),
+        1.0f);
+    const int n = __double2loint(t) & 3;
+    s_out = (n == 0) ? s : (n == 1) ? c : (n == 2) ? -s : -c;
+    c_out = (n == 0) ? c : (n == 1) ? -s : (n == 2) ? -c : s;
+}
+
 // 1 - exp(-x) for x >= 0 in FP32: the Taylor series (degree 8, nested) below
 // 0.5, where 1 - exp(-x) would cancel; 1 - expf(-x) above. Relative error
 // below 2e-7 on [1e-10, 15].

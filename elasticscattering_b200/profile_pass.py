@@ -5,7 +5,8 @@
 
 Builds the workload's impurity field on the host, uploads it, and runs
 `--passes` lifetime passes (stage a) followed by one integration (stages b, c),
-then prints the pass metrics as JSON. Meant to run under `ncu -k <kernel> -c 1`.
+then prints the pass metrics as JSON. Meant to run under
+`ncu --clock-control none -k <kernel> -c 1` (the flag leaves the GPU clocks alone).
 With --time, every pass is timed with CUDA events on the context stream and
 each lifetime variant's lifetimes are compared bit for bit.
 """

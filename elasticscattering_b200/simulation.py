@@ -313,14 +313,26 @@ class SimulationCUDA:
                                 xy[t * npos:(t + 1) * npos].copy(), Sigma(float(out[2 * t]), float(out[2 * t + 1])))
                 for t in range(nt)]
 
-    def ComputeLifetimes(self, magnetic_field: float) -> tuple[np.ndarray, dict]:
+    def ComputeLifetimes(self, magnetic_field: float, copy: bool = True) -> tuple[np.ndarray | None, dict]:
         """SimulationCL::ComputeLifetimes (src/sim/SimulationCL.cpp:113-177) with the
-        raw lifetimes copied out ([j][i][q][p] order) and the metrics."""
-        out = np.zeros(self.n_orbits)
+        raw lifetimes copied out ([j][i][q][p] order) and the metrics. copy=False
+        leaves them on the device only (ReadLifetimes reads a range)."""
+        out = np.zeros(self.n_orbits) if copy else None
         m = Metrics()
-        self._check(N.cuda_lib().es_compute_lifetimes(self._ctx, float(magnetic_field), out.ctypes.data,
-                                                      C.byref(m)))
+        self._check(N.cuda_lib().es_compute_lifetimes(self._ctx, float(magnetic_field),
+                                                      out.ctypes.data if copy else None, C.byref(m)))
         return out, m.as_dict()
+
+    def SetRows(self, j0: int, j1: int) -> None:
+        """es_set_rows: the following passes cover start rows [j0, j1) only, and
+        their sigmas are those rows' share (shares of a row partition add up)."""
+        self._check(N.cuda_lib().es_set_rows(self._ctx, int(j0), int(j1)))
+
+    def ReadLifetimes(self, first: int, count: int) -> np.ndarray:
+        """es_read_lifetimes: `count` resident lifetimes from orbit `first` on."""
+        out = np.zeros(int(count))
+        self._check(N.cuda_lib().es_read_lifetimes(self._ctx, int(first), int(count), out.ctypes.data))
+        return out
 
     def DeriveTemperatures(self, temperatures) -> list[Sigma]:
         ts = np.ascontiguousarray(temperatures, dtype=np.float64)
@@ -333,6 +345,13 @@ class SimulationCUDA:
         ts = np.ascontiguousarray(temperatures, dtype=np.float64)
         self._check(N.cuda_lib().es_enqueue_sigmas(self._ctx, float(magnetic_field), ts.ctypes.data, len(ts),
                                                    C.c_void_p(d_out_ptr)))
+
+    def enqueue_derive_temperatures(self, temperatures: np.ndarray, d_out_ptr: int) -> None:
+        """es_enqueue_derive_temperatures: stages (b)+(c) on the resident lifetimes,
+        2*n_t doubles to device memory, no host wait."""
+        ts = np.ascontiguousarray(temperatures, dtype=np.float64)
+        self._check(N.cuda_lib().es_enqueue_derive_temperatures(self._ctx, ts.ctypes.data, len(ts),
+                                                                C.c_void_p(d_out_ptr)))
 
     def synchronize(self) -> None:
         self._check(N.cuda_lib().es_synchronize(self._ctx))

@@ -180,4 +180,83 @@ def shard_samples(wl: BatchWorkload, rank: int, world: int, per_rank: int) -> Ba
     return out
 
 
+def representative_slice(wl: BatchWorkload, k: int = 0) -> BatchWorkload:
+    """Three samples of the draw, one per start grid -- the k-th 129^2, the k-th
+    257^2 and the k-th 513^2 sample -- with every field and temperature. The
+    draw picks each start grid with probability 1/3, so this slice holds the
+    orbits of three average samples; slices k = 0, 1, ... are disjoint (the
+    per-GPU work of a weak-scaling run)."""
+    import copy
+    picked = []
+    for d in sorted({s.dim for s in wl.samples}):
+        of_dim = [s for s in wl.samples if s.dim == d]
+        if k >= len(of_dim):
+            raise ValueError(f"the draw holds {len(of_dim)} samples of {d}^2 start positions; slice {k} requested")
+        picked.append(of_dim[k])
+    out = copy.copy(wl)
+    out.samples = picked
+    out.name = f"{wl.name.split('-')[0]}-slice{k}-{len(picked)}x{len(wl.fields)}x{len(wl.temperatures)}"
+    return out
+
+
+def expected_cells(density: float, impurity_radius: float, magnetic_field: float, cell_size: float,
+                   speed: float = 1.68e5) -> float:
+    """Cell steps an orbit takes on average before its first impurity hit: the
+    straight-line mean free path 1 / (2 r_i n), capped by the orbit's
+    circumference 2 pi v m* / (e B), in cells, plus the start cell."""
+    import math
+    mfp = 1.0 / (2.0 * impurity_radius * density)
+    circ = 2.0 * math.pi * speed * M_EFF / (E_CHARGE * magnetic_field)
+    return 1.0 + min(mfp, circ) / cell_size
+
+
+def sample_cost(wl: BatchWorkload, s: SweepSample) -> float:
+    """Estimated cost of one sample's sweep: orbits x expected cell steps, summed
+    over the fields and both sectors (the walk dominates every pass)."""
+    import math
+    n_imp = s.density * (wl.region_size + 2 * wl.region_extends) ** 2
+    cpr = max(1, round(math.sqrt(n_imp / wl.target_cell_population)))
+    cell = (wl.region_size + 2 * wl.region_extends) / cpr
+    orbits = s.dim * s.dim * 4 * wl.phi_steps
+    return sum(2 * orbits * expected_cells(s.density, wl.impurity_radius, b, cell, wl.particle_speed)
+               for b in wl.fields)
+
+
+def lpt_partition(costs: list, world: int) -> list:
+    """Longest processing time first: items in decreasing cost (ties by index)
+    go to the rank with the smallest load so far (ties to the lowest rank).
+    Returns, per rank, the item indices in increasing order. Deterministic."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
+def lpt_shard(wl: BatchWorkload, rank: int, world: int) -> BatchWorkload:
+    """The samples rank `rank` runs when the whole draw is split over `world`
+    GPUs by LPT on sample_cost (strong scaling: the total work is fixed)."""
+    import copy
+    if not 0 <= rank < world:
+        raise ValueError("bad shard")
+    parts = lpt_partition([sample_cost(wl, s) for s in wl.samples], world)
+    out = copy.copy(wl)
+    out.samples = [wl.samples[i] for i in parts[rank]]
+    out.name = f"{wl.name.split('-')[0]}-lpt{rank}of{world}-{len(out.samples)}x{len(wl.fields)}x{len(wl.temperatures)}"
+    return out
+
+
+def row_split(dim: int, rank: int, world: int) -> tuple:
+    """Start rows [j0, j1) of one sector pass that rank `rank` of `world` GPUs
+    computes when a single pass is split (the rows hold equal orbit counts)."""
+    if not 0 <= rank < world or world > dim:
+        raise ValueError("bad row split")
+    return (rank * dim) // world, ((rank + 1) * dim) // world
+
+
 WORKLOADS = {"config0": config0, "config1": config1, "config3": config3}

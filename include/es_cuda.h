@@ -121,6 +121,17 @@ es_status es_set_tuning(es_ctx* ctx, const es_tuning* tuning);
  * for failures of es_create and es_derive_temperatures_noalloc. */
 const char* es_last_error(const es_ctx* ctx);
 
+/* Restricts the following passes of this context to start rows [j0, j1)
+ * (0 <= j0 < j1 <= positions_per_row; the default is every row). Stage (a)
+ * traces only those rows' orbits, whose lifetimes land at their usual place in
+ * the pass's [j][i][q][p] order, and stages (b)+(c) return those rows' share of
+ * sigma. The shares of a partition of the rows add up to the whole pass's
+ * sigma: a sector pass too large for one GPU is split over GPUs this way, each
+ * computing a row range, the shares summed in rank order. No reference
+ * counterpart (the reference runs every pass on one device). The images path
+ * (es_compute_sigmas_images) and es_average_lifetime need every row. */
+es_status es_set_rows(es_ctx* ctx, int32_t j0, int32_t j1);
+
 /* Replaces the impurity/index upload in SimulationCL::ComputeLifetimes
  * (src/sim/SimulationCL.cpp:119-125). imp_xy holds n_indexed ordered
  * impurities as x,y pairs (Grid::GetImpurities, src/sim/Grid.h:74), cell_end
@@ -160,6 +171,12 @@ es_status es_compute_sigmas_images(es_ctx* ctx, double magnetic_field, const dou
  * es_derive_temperatures. */
 es_status es_compute_lifetimes(es_ctx* ctx, double magnetic_field, double* out_lifetimes, es_metrics* out_metrics);
 
+/* Copies `count` raw lifetimes of the resident pass, starting at orbit `first`
+ * ([j][i][q][p] order), to the host array out. No reference counterpart (the
+ * reference reads whole buffers back, src/sim/SimulationCL.cpp:148); it reads
+ * a band of start rows of a pass too large to copy out whole. */
+es_status es_read_lifetimes(es_ctx* ctx, int64_t first, int64_t count, double* out);
+
 /* Replaces the temperature loop of SimulationCL::ComputeSigmas
  * (src/sim/SimulationCL.cpp:82-84, DeriveTemperature :179-189) on the
  * lifetimes resident from the last es_compute_lifetimes. */
@@ -171,6 +188,11 @@ es_status es_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_
  * until es_read_metrics. No host synchronisation. */
 es_status es_enqueue_sigmas(es_ctx* ctx, double magnetic_field, const double* temperatures, int32_t n_t,
                             double* d_out_sigma);
+
+/* Asynchronous form of es_derive_temperatures: enqueues stages (b)+(c) for
+ * every temperature on the resident lifetimes and writes 2*n_t doubles to the
+ * DEVICE pointer d_out_sigma. No host synchronisation. */
+es_status es_enqueue_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_t n_t, double* d_out_sigma);
 
 /* Asynchronous stage (a) only: enqueues the lifetime pass for field B on the
  * context stream (SimulationCL::ComputeLifetimes without its blocking copies,
@@ -224,16 +246,24 @@ es_status es_debug_trace(es_ctx* ctx, double px, double py, int32_t q, int32_t p
  * sector's settings, field and temperatures, and d_out_sigma (device memory,
  * 2 * n_t doubles: xx, xy per temperature). Work is enqueued on `stream`
  * (a cudaStream_t; NULL = the legacy default stream) and not waited for.
+ * Every argument (each temperature included) is checked before anything is
+ * enqueued: an error return means no work was queued and d_out_sigma is
+ * untouched. n_t == 0 enqueues nothing.
+ *
+ * Results agree with es_derive_temperatures to about 1e-12 relative, not bit
+ * for bit: this entry point builds its phase table on the device (device
+ * cos/sin), the allocating path on the host (host libm).
  *
  * The scratch (phase table and block partial sums) is one fixed array of
  * 169 KB that every GPU which loads this library holds until the process
  * exits. Limit: phi_steps <= 1025; larger values return ES_ERR_BAD_ARG with a
- * message in es_last_error(NULL). The first call on a device (with that device
- * current) looks up the array's device address; make it before any stream
- * capture. Every call shares the array and leaves its contents behind; each
- * call rewrites every slot it reads before reading it, so nothing needs
- * clearing between calls, but calls whose work overlaps on the GPU (different
- * streams, or threads) race on it. */
+ * message in es_last_error(NULL). The first call in a CUDA context (with that
+ * context's device current) looks up the array's device address in that
+ * context and caches it under the context's id; make that first call before
+ * any stream capture. Every call shares the array and leaves its contents
+ * behind; each call rewrites every slot it reads before reading it, so nothing
+ * needs clearing between calls, but calls whose work overlaps on the GPU
+ * (different streams, or threads) race on it. */
 es_status es_derive_temperatures_noalloc(const double* d_lifetimes, int32_t positions_per_row, int32_t phi_steps,
                                          const es_settings* s, int32_t coherent, double magnetic_field,
                                          const double* temperatures, int32_t n_t, double* d_out_sigma,

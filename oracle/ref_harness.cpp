@@ -161,7 +161,9 @@ int ref_sim_lifetimes(void* p, double magnetic_field, double* out, int* metrics7
 
 /* The body of SimulationCPU::ComputeLifetimes (src/sim/SimulationCPU.cpp:105-135)
  * restricted to start-position rows [j0, j1): used to time a bounded sample of a
- * large sector pass on the CPU. Writes (j1-j0)*dim*4*ppq lifetimes. */
+ * large sector pass on the CPU, and to split a pass over many processes. Writes
+ * (j1-j0)*dim*4*ppq lifetimes and the rows' counters, the per-orbit maxima
+ * included. */
 long long ref_sim_lifetimes_rows(void* p, double magnetic_field, int j0, int j1, double* out, int* metrics7)
 {
     RefSim* rs = (RefSim*)p;
@@ -176,9 +178,15 @@ long long ref_sim_lifetimes_rows(void* p, double magnetic_field, int j0, int j1,
             for (int q = 0; q < 4; q++) {
                 for (int pp = 0; pp < s.ss.particles_per_quadrant; pp++) {
                     auto particle = CreateParticle(q, pp, position, &s.ps);
+                    const int last_cells = pm.cells_passed, last_tested = pm.impurities_tested;
                     double lt = TraceOrbit(&particle, &s.is, rs->grid->GetImpurities(), rs->grid->GetIndex(), pm);
                     if (out) out[k] = lt;
                     k++;
+                    /* the per-orbit maxima, as src/sim/SimulationCPU.cpp:123-131 keeps them */
+                    if (pm.max_cells_passed < pm.cells_passed - last_cells)
+                        pm.max_cells_passed = pm.cells_passed - last_cells;
+                    if (pm.max_impurities_tested < pm.impurities_tested - last_tested)
+                        pm.max_impurities_tested = pm.impurities_tested - last_tested;
                 }
             }
         }

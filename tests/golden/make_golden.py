@@ -3,7 +3,9 @@
 Run here, where the reference tree and its CPU build (oracle/_ref, see
 oracle/Makefile) exist:
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
+
+REFERENCE_ROOT is the root of the reference's source tree (required).
 
 It writes
   sigma_tables.json     the golden sigma rows of the reference's integration test
@@ -178,7 +180,9 @@ def ref_outputs(tables: dict, imps: dict) -> dict:
 
 
 def main() -> None:
-    ref_root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT")
+    ref_root = Path(sys.argv[1])
     imps = {}
     for name in ("test_impurities.dat", "real_case_impurities.dat", "test_impurities_lt.dat"):
         a = read_dat(ref_root / "tests/data" / name)

@@ -47,3 +47,20 @@ def test_roofline_figures_come_from_the_committed_profiles():
     full = bench.profiled_traffic("split", 34_081_284)
     half = bench.profiled_traffic("split", 34_081_284 // 2)
     assert abs(full - 2 * half) / full < 1e-6
+
+
+def test_reference_arm_default_is_the_config2_slice():
+    """The driver's reference arm (no --workload) times the reference's CPU code on
+    the same workload as the GPU arm's default: the config-2 sweep slice."""
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0",
+                        "--ref-rows", "1"], cwd=ROOT, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.strip()]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    if "unavailable" in d:
+        return
+    assert d["config"]["workload"] == "config2-slice0-3x32x3"
+    assert d["value"] > 0 and d["sigma_points_per_sec"] > 0
+    assert d["e2e"]["value"] == d["value"]

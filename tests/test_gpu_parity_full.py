@@ -1,0 +1,215 @@
+"""Full-size parity of the CUDA path with the reference's own CPU build.
+
+The workloads the bench runs, checked against the reference's SimulationCPU
+(oracle/_ref/libes_ref.so, spread over processes by tests/ref_pool.py) on the
+same seeded inputs, at their full sizes:
+
+- 257^2 x 516 orbits, 5e15 m^-2: every orbit of every start row, all five fields
+  (1, 5, 10, 20, 40 T) and both sectors;
+- one 513^2 sample of the 64-sample sweep (the first 513^2 draw) at its smallest,
+  middle and largest field, per pass and through the batched graph replay;
+- 1025^2 x 1028 orbits, 1e16 m^-2, r_i 5 nm, B = 40 T: three bands of 16 start
+  rows of the full-size pass, and sigma at 129^2 start positions.
+
+Bars (north star): the same hit/no-hit decision for every orbit, sigma within
+1e-9 relative on the plain FP64 path and within 1e-6 on the FP32/FP64 split
+path. Per-orbit lifetimes are additionally held to 1e-9 relative on both paths
+(the split path recomputes every winning crossing with the FP64 arithmetic),
+and the reference's metric counters must be equal.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from elasticscattering_b200 import Grid, SimulationCUDA, make_settings, workloads
+from elasticscattering_b200 import _native as N
+from elasticscattering_b200.batch import BatchPass, BatchSweep
+from ref_pool import RefPool, spec_of
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref (the reference's CPU build) is absent")]
+
+SIGMA_RTOL = {N.ES_PRECISION_FP64: 1e-9, N.ES_PRECISION_SPLIT: 1e-6}
+LIFETIME_RTOL = 1e-9
+TEMPS = [1e-3, 4.0, 40.0]
+COUNTERS = ("cells_passed", "impurities_tested", "particles_inside_impurity", "particles_escaped",
+            "particles_at_bound", "max_impurities_tested", "max_cells_passed")
+E = 1.60217646e-19
+M = 5.0 * 9.10938188e-31
+HALF_PI = 1.570796326794896619231
+
+
+@pytest.fixture(scope="module")
+def ref_pool():
+    pool = RefPool()
+    yield pool
+    pool.close()
+
+
+def phase_bound_times(alpha: float, clockwise: bool, ppq: int, coherent: bool, B: float) -> np.ndarray | None:
+    """GetBoundTime per phase of the incoherent sector (src/sim/es/details.h:219-228)."""
+    if coherent:
+        return None
+    omega = E * B / M
+    step = alpha * 2.0 / (ppq - 1)
+    out = np.empty(4 * ppq)
+    for q in range(4):
+        for p in range(ppq):
+            phi = -alpha + q * HALF_PI + p * step
+            rem = (phi + alpha) - HALF_PI * np.floor((phi + alpha) / HALF_PI)
+            out[q * ppq + p] = (rem if clockwise else (2.0 * alpha - rem)) / omega
+    return out
+
+
+def compare(gpu: np.ndarray, ref: np.ndarray, phase_bound: np.ndarray | None) -> dict:
+    """Per-orbit comparison in row-sized pieces: class flips (0 = no lifetime,
+    1 = hit, 2 = clamped to the sector bound), max relative lifetime difference
+    over orbits of equal class, and the bit-identical fraction."""
+    n = len(ref)
+    per = len(phase_bound) if phase_bound is not None else 1
+    step = per * max(1, (1 << 22) // per)
+    flips, max_rel, same = 0, 0.0, 0
+    for a in range(0, n, step):
+        g, r = gpu[a:a + step], ref[a:a + step]
+        cg = np.where(g == 0, 0, 1)
+        cr = np.where(r == 0, 0, 1)
+        if phase_bound is not None:
+            bt = np.tile(phase_bound, len(r) // per)
+            cg = np.where((g != 0) & (g == bt), 2, cg)
+            cr = np.where((r != 0) & (r == bt), 2, cr)
+        flips += int((cg != cr).sum())
+        nz = (r != 0) & (cg == cr)
+        if nz.any():
+            max_rel = max(max_rel, float((np.abs(g[nz] - r[nz]) / np.abs(r[nz])).max()))
+        same += int((g.view(np.int64) == r.view(np.int64)).sum())
+    return {"flips": flips, "max_rel": max_rel, "bit_identical": same / n}
+
+
+def check_pass(tag, gpu_lt, gpu_m, gpu_sig, res, precision, phase_bound, temps=TEMPS):
+    r = compare(gpu_lt, res.lifetimes(), phase_bound)
+    assert r["flips"] == 0, (tag, r)
+    assert r["max_rel"] <= LIFETIME_RTOL, (tag, r)
+    for k in COUNTERS:
+        assert gpu_m[k] == res.metrics[k], (tag, k, gpu_m[k], res.metrics[k])
+    if gpu_sig is not None:
+        tol = SIGMA_RTOL[precision]
+        for T, s in zip(temps, gpu_sig):
+            xx, xy = res.sigmas[T]
+            assert abs(s.xx - xx) <= tol * abs(xx) and abs(s.xy - xy) <= tol * abs(xy), (tag, T, s, (xx, xy))
+    return r
+
+
+def settings_of(w, density=None):
+    return make_settings(w.tau, w.alpha, w.clockwise, w.particle_speed, w.region_size, w.region_extends,
+                         w.density if density is None else density, w.impurity_radius, w.target_cell_population)
+
+
+def test_config1_every_orbit_all_fields(cuda_device, ref_pool):
+    """257^2 x 516, 5e15 m^-2: all 10 sector passes, every orbit, both precisions."""
+    w = workloads.config1()
+    passes = [spec_of(w, w.seed(0), coh, B) for B in w.fields for coh in (True, False)]
+    results = ref_pool.run(passes, temperatures=TEMPS)
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    s = settings_of(w)
+    for precision in (N.ES_PRECISION_FP64, N.ES_PRECISION_SPLIT):
+        with SimulationCUDA(w.dim, w.phi_steps, g.info(), device=cuda_device, precision=precision) as sim:
+            for res in results:
+                sp = res.spec
+                sim.InitSample(g, s, sp.coherent)
+                lt, m = sim.ComputeLifetimes(sp.field_b)
+                sig = sim.DeriveTemperatures(TEMPS)
+                check_pass(("config1", precision, sp.field_b, sp.coherent), lt, m, sig, res, precision,
+                           phase_bound_times(w.alpha, w.clockwise, w.phi_steps, sp.coherent, sp.field_b))
+    ref_pool.discard(results)
+
+
+def test_config2_largest_sample_three_fields(cuda_device, ref_pool):
+    """The first 513^2 sample of the 64-sample draw at B = 1, 19.87 and 40 T: per-pass
+    FP64 and split against the reference per orbit, and the batched graph replay's
+    sigma (split, the library's default mode) against the reference's sigma."""
+    wl = workloads.config2()
+    sample = next(sm for sm in wl.samples if sm.dim == 513)
+    fields = [wl.fields[0], wl.fields[len(wl.fields) // 2], wl.fields[-1]]
+    w = workloads.config1()
+    w.region_extends, w.dim, w.density = wl.region_extends, sample.dim, sample.density
+    passes = [spec_of(w, sample.seed, coh, B) for B in fields for coh in (True, False)]
+    results = ref_pool.run(passes, temperatures=TEMPS)
+    g = Grid.from_seed(sample.seed, wl.region_size, wl.region_extends, sample.density, wl.impurity_radius,
+                       wl.target_cell_population)
+    s = settings_of(w)
+    for precision in (N.ES_PRECISION_FP64, N.ES_PRECISION_SPLIT):
+        with SimulationCUDA(w.dim, w.phi_steps, g.info(), device=cuda_device, precision=precision) as sim:
+            for res in results:
+                sp = res.spec
+                sim.InitSample(g, s, sp.coherent)
+                lt, m = sim.ComputeLifetimes(sp.field_b)
+                sig = sim.DeriveTemperatures(TEMPS)
+                check_pass(("config2", sample.index, precision, sp.field_b, sp.coherent), lt, m, sig, res,
+                           precision, phase_bound_times(w.alpha, w.clockwise, w.phi_steps, sp.coherent, sp.field_b))
+                del lt
+    with BatchSweep(cuda_device) as b:
+        gid = b.add_grid(g)
+        b.set_passes([BatchPass(gid, w.dim, w.phi_steps, r.spec.coherent, w.region_size, g.info().cell_size,
+                                r.spec.field_b, s, TEMPS) for r in results])
+        out, mets = b.run()
+    tol = SIGMA_RTOL[N.ES_PRECISION_SPLIT]
+    for k, res in enumerate(results):
+        for t, T in enumerate(TEMPS):
+            xx, xy = res.sigmas[T]
+            assert abs(out[k, t, 0] - xx) <= tol * abs(xx) and abs(out[k, t, 1] - xy) <= tol * abs(xy), \
+                ("batched", res.spec.field_b, res.spec.coherent, T)
+        for c in ("cells_passed", "impurities_tested", "particles_inside_impurity", "particles_escaped",
+                  "particles_at_bound"):
+            assert mets[k][c] == res.metrics[c], ("batched", k, c)
+    ref_pool.discard(results)
+
+
+def test_config3_full_size_row_bands(cuda_device, ref_pool):
+    """1025^2 x 1028 orbits per pass (1.08 G), B = 40 T: the whole pass on the GPU,
+    three bands of 16 start rows (first, middle, last) against the reference."""
+    w = workloads.config3()
+    bands = [(0, 16), (w.dim // 2 - 8, w.dim // 2 + 8), (w.dim - 16, w.dim)]
+    per_row = w.dim * 4 * w.phi_steps
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    s = settings_of(w)
+    B = w.fields[0]
+    for coh in (True, False):
+        spec = spec_of(w, w.seed(0), coh, B)
+        refs = [ref_pool.run([spec], rows=band)[0] for band in bands]
+        pb = phase_bound_times(w.alpha, w.clockwise, w.phi_steps, coh, B)
+        for precision in (N.ES_PRECISION_FP64, N.ES_PRECISION_SPLIT):
+            with SimulationCUDA(w.dim, w.phi_steps, g.info(), device=cuda_device, precision=precision) as sim:
+                sim.InitSample(g, s, coh)
+                _, m = sim.ComputeLifetimes(B, copy=False)
+                assert m["particles_escaped"] == 0
+                for band, res in zip(bands, refs):
+                    lt = sim.ReadLifetimes(band[0] * per_row, (band[1] - band[0]) * per_row)
+                    r = compare(lt, res.lifetimes(), pb)
+                    assert r["flips"] == 0 and r["max_rel"] <= LIFETIME_RTOL, (coh, precision, band, r)
+        ref_pool.discard(refs)
+
+
+def test_config3_sigma_at_reduced_dim(cuda_device, ref_pool):
+    """The config-3 geometry (1e16 m^-2, r_i 5 nm, 1028 phases, B = 40 T) at 129^2
+    start positions: every orbit and sigma against the reference."""
+    w = workloads.config3()
+    dim = 129
+    passes = [spec_of(w, w.seed(0), coh, w.fields[0], dim=dim) for coh in (True, False)]
+    results = ref_pool.run(passes, temperatures=TEMPS)
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    s = settings_of(w)
+    for precision in (N.ES_PRECISION_FP64, N.ES_PRECISION_SPLIT):
+        with SimulationCUDA(dim, w.phi_steps, g.info(), device=cuda_device, precision=precision) as sim:
+            for res in results:
+                sp = res.spec
+                sim.InitSample(g, s, sp.coherent)
+                lt, m = sim.ComputeLifetimes(sp.field_b)
+                sig = sim.DeriveTemperatures(TEMPS)
+                check_pass(("config3-129", precision, sp.coherent), lt, m, sig, res, precision,
+                           phase_bound_times(w.alpha, w.clockwise, w.phi_steps, sp.coherent, sp.field_b))
+    ref_pool.discard(results)
