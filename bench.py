@@ -733,7 +733,7 @@ def run_batched(args) -> None:
         # per pass: orbit table, lifetime walk, FP64 re-trace, integration, reduction
         kernels_per_replay = 5 * n_pass
     else:
-        kernels_per_replay = (n_pass if tune.shape["mode"] == N.ES_BATCH_PASS_NODES else 1) + 1
+        kernels_per_replay = 2  # the persistent kernel and the FP64 re-trace
     alg_flops = sum(lifetime_flops(m, 0) for m in mets) + FLOP_MODEL["per_orbit"] * orbits
     retraced = sum(m["retraced_fp64"] for m in mets)
 

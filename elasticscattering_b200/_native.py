@@ -62,8 +62,6 @@ class Tuning(C.Structure):
 
 
 ES_BATCH_MAX_T = 8
-ES_BATCH_PASS_NODES = 0
-ES_BATCH_GRID = 1
 ES_BATCH_PERSISTENT = 2
 ES_BATCH_PASS_KERNELS = 3
 

@@ -43,12 +43,10 @@ SHAPE_CANDIDATES = (
     {"mode": N.ES_BATCH_PERSISTENT, "blocks_per_sm": 4, "chunk_iters": 32},
     {"mode": N.ES_BATCH_PERSISTENT, "blocks_per_sm": 4, "chunk_iters": 64},
     {"mode": N.ES_BATCH_PERSISTENT, "blocks_per_sm": 3, "chunk_iters": 32},
-    {"mode": N.ES_BATCH_PASS_NODES, "blocks_per_sm": 4, "chunk_iters": 32},
-    {"mode": N.ES_BATCH_GRID, "blocks_per_sm": 4, "chunk_iters": 32},
     {"mode": N.ES_BATCH_PASS_KERNELS, "blocks_per_sm": 4, "chunk_iters": 32},
 )
 PILOT_DIM = 65
-TUNER_VERSION = 2
+TUNER_VERSION = 3
 
 
 def default_cache() -> Path:

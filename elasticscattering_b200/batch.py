@@ -5,10 +5,10 @@ src/SimulationRunner.cpp:86-151): per sample one Grid, per field and sector one
 Simulation::ComputeSigmas call. `BatchSweep` takes the whole list of those calls
 at once and runs them through the es_batch_* C ABI (include/es_cuda.h),
 recorded once as a CUDA graph and replayed. The default mode
-(ES_BATCH_PASS_KERNELS) runs the single-pass kernels for each pass in turn; the
-other modes fuse stages (b) and (c) into one lifetime kernel over all passes
-(ES_BATCH_PERSISTENT and the rest). Each pass returns what ComputeSigmas
-returns for it (one Sigma per temperature) plus its metrics.
+(ES_BATCH_PASS_KERNELS) runs the single-pass kernels for each pass in turn;
+ES_BATCH_PERSISTENT fuses stages (b) and (c) into one persistent lifetime kernel
+over all passes (faster for sweeps of many small passes). Each pass returns what
+ComputeSigmas returns for it (one Sigma per temperature) plus its metrics.
 """
 from __future__ import annotations
 

@@ -5,9 +5,13 @@
 // pass in turn the single-pass path's kernels (es_lifetime_split.cu or
 // es_lifetime_fp64.cu, then es_integrate.cu) on shared device scratch: the
 // lean lifetime kernel without the integrand is 12-16% faster on B200 than the
-// fused kernels below, and the 16 bytes per orbit it moves through HBM are ~1%
-// of its time. The other modes fuse stages (b) and (c) into the lifetime
-// kernel, as described next.
+// fused kernel below on passes of 129^2 start positions and up, and the 16
+// bytes per orbit it moves through HBM are ~1% of its time. ES_BATCH_PERSISTENT
+// fuses stages (b) and (c) into one persistent lifetime kernel over every pass,
+// as described next; it wins on sweeps of many small passes (the surrogate's
+// training runs of 65^2 x 100 orbits), where per-pass launches dominate. Two
+// block-per-work-item modes (one grid over every pass, one graph node per pass)
+// never won on B200 and were removed.
 //
 // No reference counterpart: the reference runs one pass at a time
 // (SimulationRunner::RunSample, src/SimulationRunner.cpp:103-151, calling
@@ -307,185 +311,6 @@ __global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks) batch_kernel(Bat
     }
 }
 
-// One block = one work item of 256 consecutive orbits of one pass (one orbit
-// per thread): a thread holds no loop state across its walk, as in the
-// single-pass kernels. The block ends with a fixed-order reduction and one
-// fixed-point atomic per sum. I is the pass record and f reads the walk's
-// constants from it (kernel parameter or shared memory).
-template <int kPrec, class F>
-__device__ __forceinline__ void block_item(const BatchInstanceD& I, const F& f, const BatchLaunch& B, long long pass,
-                                           long long item_in_pass)
-{
-    __shared__ double s_sum[kBatchWarps][2 * kBatchMaxTau];
-    __shared__ unsigned s_met[kBatchWarps][kMetCount];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-    const long long g = item_in_pass * (kBatchWarps * 32) + threadIdx.x;
-    const bool active = g < I.L.n_orbits;
-    unsigned cells = 0, imps = 0, cross = 0, starts = 0;
-    int flags = kTraceOk;
-    bool retrace = false;
-    double lt = 0.0;
-    if (active) {
-        if (kPrec == ES_PRECISION_SPLIT) {
-            SplitCounters sc;
-            retrace = split_orbit(f, g, sc, flags, lt);
-            cells = sc.cells, imps = sc.imps, cross = sc.crossings, starts = sc.start_tests;
-        } else {
-            OrbitCounters oc;
-            lt = fp64_lifetime(I.L, g, &oc, &flags);
-            cells = oc.cells, imps = oc.imps, cross = oc.crossings, starts = oc.start_tests;
-        }
-    }
-
-    // this orbit's Simpson-weighted kernel values, per relaxation time
-    double val[2 * kBatchMaxTau];
-#pragma unroll
-    for (int k = 0; k < 2 * kBatchMaxTau; k++) val[k] = 0.0;
-    if (active && !retrace) {
-        const int n_phase = I.L.n_phase, dim = I.L.dim;
-        const int v = (int)(g % n_phase);
-        const long long pidx = g / n_phase;
-        const int i = (int)(pidx % dim);
-        const int j = (int)(pidx / dim);
-        const double wpos = simpson_w(j, dim) * simpson_w(i, dim);
-        const PhaseSigma ph = I.phase_sigma[v];
-        if (kPrec == ES_PRECISION_SPLIT) {
-            const double wgt = wpos * ph.weight;
-#pragma unroll
-            for (int k = 0; k < kBatchMaxTau; k++) {
-                if (k < I.n_tau) {
-                    float r_xx, r_xy;
-                    kernel_fp32(I, k, lt, ph, r_xx, r_xy);
-                    val[2 * k] = wgt * (double)r_xx;
-                    val[2 * k + 1] = wgt * (double)r_xy;
-                }
-            }
-        } else {
-            double sa_raw, ca_raw;
-            sincos(ph.phi + I.w_signed * lt, &sa_raw, &ca_raw);
-#pragma unroll
-            for (int k = 0; k < kBatchMaxTau; k++) {
-                if (k < I.n_tau) {
-                    const bool keep = lt < I.max_lt[k];
-                    const double t = keep ? lt : I.max_lt[k];
-                    double sa = sa_raw, ca = ca_raw;
-                    if (!keep) sincos(ph.phi + I.w_signed * t, &sa, &ca);
-                    const double z = exp(-t / I.tau[k]);
-                    double r = ph.cos_phi - ca * z;
-                    r += I.wtau[k] * sa * z;
-                    r -= I.wtau[k] * ph.sin_phi;
-                    val[2 * k] = ((r * ph.cos_phi) * ph.weight) * wpos;
-                    val[2 * k + 1] = ((r * ph.sin_phi) * ph.weight) * wpos;
-                }
-            }
-        }
-    }
-    if (kPrec == ES_PRECISION_SPLIT) {
-        const unsigned want = __ballot_sync(0xffffffffu, retrace);
-        if (want) {
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(B.retrace_count, (unsigned long long)__popc(want));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (retrace) {
-                const unsigned long long slot = base + __popc(want & ((1u << lane) - 1u));
-                if (slot < (unsigned long long)B.retrace_cap)
-                    B.retrace[slot] = ((unsigned long long)pass << kRetraceOrbitBits) | (unsigned long long)g;
-                else
-                    atomicOr(B.error, kErrRetraceOverflow);
-            }
-        }
-    }
-
-    // block reduction: fixed shuffle tree per warp, then warps in order
-#pragma unroll
-    for (int k = 0; k < 2 * kBatchMaxTau; k++) {
-        if (k < 2 * I.n_tau) {
-            const double s = warp_sum_d(val[k]);
-            if (lane == 0) s_sum[warp][k] = s;
-        }
-    }
-    {
-        const unsigned m[kMetCount] = {
-            __reduce_add_sync(0xffffffffu, cells),
-            __reduce_add_sync(0xffffffffu, imps),
-            __reduce_add_sync(0xffffffffu, (flags & kTraceInside) ? 1u : 0u),
-            __reduce_add_sync(0xffffffffu, (flags & kTraceEscaped) ? 1u : 0u),
-            __reduce_add_sync(0xffffffffu, (flags & kTraceAtBound) ? 1u : 0u),
-            __reduce_max_sync(0xffffffffu, imps),
-            __reduce_max_sync(0xffffffffu, cells),
-            __reduce_add_sync(0xffffffffu, cross),
-            __reduce_add_sync(0xffffffffu, starts),
-            0u};
-        static_assert(kMetCells == 0 && kMetImps == 1 && kMetInside == 2 && kMetEscaped == 3 && kMetAtBound == 4 &&
-                          kMetMaxImps == 5 && kMetMaxCells == 6 && kMetCrossings == 7 && kMetStartTests == 8 &&
-                          kMetRetraced == 9 && kMetCount == 10,
-                      "metric slot order");
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < kMetCount; k++) s_met[warp][k] = m[k];
-        }
-    }
-    __syncthreads();
-    const int t = threadIdx.x;
-    if (t < 2 * I.n_tau) {
-        double s = 0.0;
-#pragma unroll
-        for (int w = 0; w < kBatchWarps; w++) s += s_sum[w][t];
-        const long long q = __double2ll_rn(s * I.fx_scale);
-        if (q != 0) atomicAdd(I.acc + t, (unsigned long long)q);
-    } else if (t >= 32 && t < 32 + kMetCount) {
-        const int k = t - 32;
-        unsigned long long s = 0;
-        const bool is_max = (k == kMetMaxCells || k == kMetMaxImps);
-#pragma unroll
-        for (int w = 0; w < kBatchWarps; w++)
-            s = is_max ? max(s, (unsigned long long)s_met[w][k]) : s + s_met[w][k];
-        if (s != 0) {
-            if (is_max) atomicMax(I.metrics + k, s);
-            else atomicAdd(I.metrics + k, s);
-        }
-    }
-}
-
-// Block-per-item over the whole batch in one launch: each block finds its
-// pass by binary search and stages the pass record in shared memory.
-template <int kPrec, int kMinBlocks>
-__global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks) batch_grid_kernel(BatchLaunch B)
-{
-    __shared__ BatchInstanceD s_inst;
-    __shared__ long long s_pass;
-    const long long item = blockIdx.x;
-    if (threadIdx.x == 0) {
-        long long lo = 0, hi = *B.n_inst - 1;
-        while (lo < hi) {
-            const long long mid = (lo + hi + 1) >> 1;
-            if (B.chunk_begin[mid] <= item) lo = mid;
-            else hi = mid - 1;
-        }
-        s_pass = lo;
-    }
-    __syncthreads();
-    const long long pass = s_pass;
-    {
-        const int4* src = reinterpret_cast<const int4*>(B.inst + pass);
-        int4* dst = reinterpret_cast<int4*>(&s_inst);
-        for (int k = threadIdx.x; k < (int)(sizeof(BatchInstanceD) / 16); k += blockDim.x) dst[k] = src[k];
-    }
-    __syncthreads();
-    block_item<kPrec>(s_inst, SharedFields{&s_inst.L}, B, pass, item - s_inst.chunk_begin);
-}
-
-// Block-per-item over one pass, whose record is the kernel parameter: the
-// walk's constants are constant-bank operands, as in the single-pass kernels.
-// The batch graph holds one such kernel node per pass, on parallel branches.
-template <int kPrec, int kMinBlocks>
-__global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks)
-    batch_pass_kernel(BatchLaunch B, BatchInstanceD I, long long pass)
-{
-    block_item<kPrec>(I, LaunchFields{I.L}, B, pass, blockIdx.x);
-}
-
 // The listed orbits of a split run, in FP64 (TraceOrbit, src/sim/es/lifetime.h:78-148),
 // then integrated like every other orbit. Each warp takes a contiguous slice of
 // the list (entries are appended in roughly pass order), its lanes accumulate
@@ -565,41 +390,20 @@ __global__ void __launch_bounds__(256, 2) batch_retrace_kernel(BatchLaunch B)
 }
 
 template <int kPrec, int kMinBlocks>
-cudaError_t launch_batch_t(const BatchLaunch& B, int mode, int n_sm, long long n_items, cudaStream_t s)
+cudaError_t launch_batch_t(const BatchLaunch& B, int n_sm, cudaStream_t s)
 {
-    if (mode == ES_BATCH_PERSISTENT) batch_kernel<kPrec, kMinBlocks><<<n_sm * kMinBlocks, kBatchWarps * 32, 0, s>>>(B);
-    else batch_grid_kernel<kPrec, kMinBlocks><<<(unsigned)n_items, kBatchWarps * 32, 0, s>>>(B);
+    batch_kernel<kPrec, kMinBlocks><<<n_sm * kMinBlocks, kBatchWarps * 32, 0, s>>>(B);
     return cudaGetLastError();
 }
 
-template <int kPrec, int kMinBlocks>
-cudaError_t launch_pass_t(const BatchLaunch& B, const BatchInstanceD& I, long long pass, long long n_items,
-                          cudaStream_t s)
-{
-    batch_pass_kernel<kPrec, kMinBlocks><<<(unsigned)n_items, kBatchWarps * 32, 0, s>>>(B, I, pass);
-    return cudaGetLastError();
-}
-
-// ES_BATCH_GRID / ES_BATCH_PERSISTENT: the one kernel over every pass.
-cudaError_t launch_batch(const BatchLaunch& B, int precision, int blocks_per_sm, int mode, int n_sm,
-                         long long n_items, cudaStream_t s)
+// ES_BATCH_PERSISTENT: the one kernel over every pass.
+cudaError_t launch_batch(const BatchLaunch& B, int precision, int blocks_per_sm, int n_sm, cudaStream_t s)
 {
     if (precision == ES_PRECISION_SPLIT)
-        return (blocks_per_sm == 3) ? launch_batch_t<ES_PRECISION_SPLIT, 3>(B, mode, n_sm, n_items, s)
-                                    : launch_batch_t<ES_PRECISION_SPLIT, 4>(B, mode, n_sm, n_items, s);
-    return (blocks_per_sm == 3) ? launch_batch_t<ES_PRECISION_FP64, 3>(B, mode, n_sm, n_items, s)
-                                : launch_batch_t<ES_PRECISION_FP64, 4>(B, mode, n_sm, n_items, s);
-}
-
-// ES_BATCH_PASS_NODES: the kernel of one pass.
-cudaError_t launch_pass(const BatchLaunch& B, const BatchInstanceD& I, long long pass, long long n_items,
-                        int precision, int blocks_per_sm, cudaStream_t s)
-{
-    if (precision == ES_PRECISION_SPLIT)
-        return (blocks_per_sm == 3) ? launch_pass_t<ES_PRECISION_SPLIT, 3>(B, I, pass, n_items, s)
-                                    : launch_pass_t<ES_PRECISION_SPLIT, 4>(B, I, pass, n_items, s);
-    return (blocks_per_sm == 3) ? launch_pass_t<ES_PRECISION_FP64, 3>(B, I, pass, n_items, s)
-                                : launch_pass_t<ES_PRECISION_FP64, 4>(B, I, pass, n_items, s);
+        return (blocks_per_sm == 3) ? launch_batch_t<ES_PRECISION_SPLIT, 3>(B, n_sm, s)
+                                    : launch_batch_t<ES_PRECISION_SPLIT, 4>(B, n_sm, s);
+    return (blocks_per_sm == 3) ? launch_batch_t<ES_PRECISION_FP64, 3>(B, n_sm, s)
+                                : launch_batch_t<ES_PRECISION_FP64, 4>(B, n_sm, s);
 }
 
 // Split precision: the FP64 re-trace of the run's list.
@@ -638,11 +442,6 @@ struct es_batch {
     // measured best on B200 for passes of 129^2 to 513^2 start positions x 516 phases
     // (12-16% ahead of ES_BATCH_PERSISTENT; the autotuner may choose otherwise)
     es_batch_tuning tuning{32, 4, ES_PRECISION_SPLIT, ES_BATCH_PASS_KERNELS};
-    int64_t captured_items = -1;              // grid size recorded in the graph (ES_BATCH_GRID)
-    static constexpr int kBranches = 8;       // parallel graph branches (ES_BATCH_PASS_NODES)
-    cudaStream_t branch[kBranches] = {};
-    cudaEvent_t fork = nullptr;
-    cudaEvent_t join[kBranches] = {};
     std::vector<long long> pass_items;        // work items per pass, kernel order
 
     std::vector<es_batch_grid> grids;
@@ -802,23 +601,6 @@ es_status ensure_retrace(es_batch* b, long long want)
     return ES_OK;
 }
 
-// ES_BATCH_PASS_NODES: one kernel per pass, spread round-robin over the
-// branches forked from the capture stream, joined before the re-trace.
-cudaError_t record_pass_nodes(es_batch* b, const es::BatchLaunch& L)
-{
-    cudaError_t e = cudaEventRecord(b->fork, b->stream);
-    for (int k = 0; e == cudaSuccess && k < es_batch::kBranches; k++) e = cudaStreamWaitEvent(b->branch[k], b->fork, 0);
-    const es::BatchInstanceD* hi = reinterpret_cast<const es::BatchInstanceD*>(b->h_table + b->inst_offset);
-    for (size_t pos = 0; e == cudaSuccess && pos < b->pass_items.size(); pos++)
-        e = es::launch_pass(L, hi[pos], (long long)pos, b->pass_items[pos], b->tuning.precision,
-                            b->tuning.blocks_per_sm, b->branch[pos % es_batch::kBranches]);
-    for (int k = 0; e == cudaSuccess && k < es_batch::kBranches; k++) {
-        e = cudaEventRecord(b->join[k], b->branch[k]);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[k], 0);
-    }
-    return e;
-}
-
 // ES_BATCH_PASS_KERNELS: scratch for the largest pass (allocated before the
 // capture; the graph records the addresses).
 es_status ensure_pass_scratch(es_batch* b)
@@ -922,10 +704,8 @@ es_status capture(es_batch* b)
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_retrace_count, 0, sizeof(unsigned long long), b->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_error, 0, sizeof(int), b->stream);
     if (e == cudaSuccess) {
-        if (b->tuning.mode == ES_BATCH_PASS_NODES) e = record_pass_nodes(b, L);
-        else if (b->tuning.mode == ES_BATCH_PASS_KERNELS) e = record_pass_kernels(b);
-        else e = es::launch_batch(L, b->tuning.precision, b->tuning.blocks_per_sm, b->tuning.mode, b->n_sm,
-                                  b->total_items, b->stream);
+        if (b->tuning.mode == ES_BATCH_PASS_KERNELS) e = record_pass_kernels(b);
+        else e = es::launch_batch(L, b->tuning.precision, b->tuning.blocks_per_sm, b->n_sm, b->stream);
     }
     if (e == cudaSuccess && b->tuning.precision == ES_PRECISION_SPLIT && b->tuning.mode != ES_BATCH_PASS_KERNELS)
         e = es::launch_retrace(L, b->n_sm, b->stream);
@@ -948,7 +728,6 @@ es_status capture(es_batch* b)
     b->graph = g;
     ES_BCUDA(cudaGraphInstantiate(&b->exec, b->graph, 0), "batch graph instantiation");
     b->graph_dirty = false;
-    b->captured_items = b->total_items;
     return ES_OK;
 }
 
@@ -1006,11 +785,6 @@ es_status es_batch_create(int32_t device_ordinal, es_batch** out)
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_error, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_retrace_count, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_retrace_count, sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
-    for (int k = 0; e == cudaSuccess && k < es_batch::kBranches; k++) {
-        e = cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming);
-    }
     if (e == cudaSuccess) {
         *b->h_error = 0;
         *b->h_retrace_count = 0;
@@ -1041,11 +815,6 @@ es_status es_batch_destroy(es_batch* b)
     cudaFree(b->d_retrace_count);
     if (b->h_error) cudaFreeHost(b->h_error);
     if (b->h_retrace_count) cudaFreeHost(b->h_retrace_count);
-    for (int k = 0; k < es_batch::kBranches; k++) {
-        if (b->branch[k]) cudaStreamDestroy(b->branch[k]);
-        if (b->join[k]) cudaEventDestroy(b->join[k]);
-    }
-    if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return ES_OK;
@@ -1069,8 +838,7 @@ es_status es_batch_set_tuning(es_batch* b, const es_batch_tuning* t)
         return bfail(b, ES_ERR_BAD_ARG, "blocks_per_sm must be 3 or 4 (got %d)", t->blocks_per_sm);
     if (t->precision != ES_PRECISION_FP64 && t->precision != ES_PRECISION_SPLIT)
         return bfail(b, ES_ERR_BAD_ARG, "unknown precision %d", t->precision);
-    if (t->mode != ES_BATCH_PASS_NODES && t->mode != ES_BATCH_GRID && t->mode != ES_BATCH_PERSISTENT &&
-        t->mode != ES_BATCH_PASS_KERNELS)
+    if (t->mode != ES_BATCH_PERSISTENT && t->mode != ES_BATCH_PASS_KERNELS)
         return bfail(b, ES_ERR_BAD_ARG, "unknown batch mode %d", t->mode);
     auto item_orbits = [](const es_batch_tuning& x) {
         return x.mode == ES_BATCH_PERSISTENT ? 32LL * x.chunk_iters : 32LL * es::kBatchWarps;
@@ -1354,7 +1122,7 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
     b->total_items = items;
     b->has_instances = true;
     // pass records are kernel parameters in this mode: record the graph again
-    if (b->tuning.mode == ES_BATCH_PASS_NODES || b->tuning.mode == ES_BATCH_PASS_KERNELS) b->graph_dirty = true;
+    if (b->tuning.mode == ES_BATCH_PASS_KERNELS) b->graph_dirty = true;
     // Re-traced orbits are a small fraction (observed ~0.05%); the list starts
     // at 1/1024 of the run and grows on overflow (es_batch_collect re-runs).
     if (b->tuning.precision == ES_PRECISION_SPLIT)
@@ -1369,9 +1137,7 @@ es_status es_batch_enqueue(es_batch* b)
     if (!b->has_instances) return bfail(b, ES_ERR_BAD_ARG, "es_batch_set_instances has not been called");
     if (b->tuning.precision == ES_PRECISION_SPLIT && b->retrace_cap == 0)
         if ((st = ensure_retrace(b, b->total_orbits / 1024 + 262144)) != ES_OK) return st;
-    if (b->tuning.mode == ES_BATCH_GRID && b->total_items > 0x7fffffffLL)
-        return bfail(b, ES_ERR_BAD_ARG, "more than 2^31 - 1 work items: use another batch mode or split the batch");
-    if (b->graph_dirty || !b->exec || (b->tuning.mode == ES_BATCH_GRID && b->captured_items != b->total_items))
+    if (b->graph_dirty || !b->exec)
         if ((st = capture(b)) != ES_OK) return st;
     ES_BCUDA(cudaGraphLaunch(b->exec, b->stream), "batch graph launch");
     b->launches++;

@@ -65,7 +65,6 @@ struct es_ctx {
     double* d_pos = nullptr;          // images: 3 * pos_cap doubles
     int64_t pos_cap = 0;
     double last_w = 0;                // angular speed of the resident lifetimes
-    unsigned long long* d_work = nullptr;  // orbit counter of the refill kernel
     // split precision
     float2* d_imps32 = nullptr;            // cell-local FP32 impurities
     int64_t imps32_cap = 0;
@@ -159,7 +158,6 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.walk_cap = es::host::walk_cap_for(L.radius, L.cell_size);
     L.row0 = ctx->row0;
     L.variant = ctx->tuning.lifetime_variant;
-    L.work = ctx->d_work;
     L.imps32 = ctx->d_imps32;
     L.retrace = ctx->d_retrace;
     L.retrace_count = ctx->d_retrace_count;
@@ -311,7 +309,6 @@ void release(es_ctx* ctx)
     cudaFree(ctx->d_partial);
     cudaFree(ctx->d_sigma);
     cudaFree(ctx->d_pos);
-    cudaFree(ctx->d_work);
     cudaFree(ctx->d_imps32);
     cudaFree(ctx->d_retrace);
     cudaFree(ctx->d_retrace_count);
@@ -376,7 +373,6 @@ es_status es_create(const es_sim_desc* desc, es_ctx** out)
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_phase_sigma, sizeof(es::PhaseSigma) * n_phase);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_metrics, sizeof(unsigned long long) * es::kMetCount);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_work, sizeof(unsigned long long));
     if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT) {
         // Re-traced orbits are a small fraction (guard-band decisions); a quarter
         // of the pass is a generous bound, and overflow is reported, not ignored.
@@ -473,7 +469,7 @@ es_status es_get_tuning(const es_ctx* ctx, es_tuning* out)
 es_status es_set_tuning(es_ctx* ctx, const es_tuning* tuning)
 {
     if (!ctx || !tuning) return ES_ERR_BAD_ARG;
-    if (tuning->lifetime_variant < 0 || tuning->lifetime_variant >= es::kLifetimeVariants)
+    if (!es::lifetime_variant_known(tuning->lifetime_variant))
         return fail(ctx, ES_ERR_BAD_ARG, "unknown lifetime variant %d", tuning->lifetime_variant);
     ctx->tuning = *tuning;
     return ES_OK;

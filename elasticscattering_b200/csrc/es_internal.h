@@ -59,7 +59,6 @@ struct LifetimeLaunch {
     int cpr, dim, n_phase, clockwise, coherent, walk_cap;
     int row0;                     // first start-position row of this launch
     int variant;                  // LifetimeVariant
-    unsigned long long* work;     // refill variant: orbit counter, zeroed by the launcher
     // split precision
     const float2* imps32;         // cell-local FP32 copy of imps
     long long* retrace;           // orbits handed to the FP64 re-trace
@@ -72,16 +71,20 @@ struct LifetimeLaunch {
     double4* orbit_table;
 };
 
+// FP64 lifetime kernel choices (es_tuning.lifetime_variant). The values 1, 3,
+// 4 and 5 named variants that measured slower on B200 and were removed (lane
+// refill, 19.8 ms against 15.3 ms per 257^2 x 516 pass; lanes over
+// neighbouring positions, 55 ms); es_set_tuning rejects them.
 enum LifetimeVariant : int {
     kLifetimePerThread = 0,      // one orbit per thread, <= 80 registers (3 blocks of 256 per SM)
-    kLifetimeRefill = 1,         // persistent warps, lanes refill as their orbits finish, 2 blocks per SM
     kLifetimePerThreadLean = 2,  // one orbit per thread, <= 64 registers (4 blocks per SM)
-    kLifetimeRefillLean = 3,     // lane refill, <= 85 registers (3 blocks per SM)
-    kLifetimePositionMajor = 4,  // as 2, lanes = neighbouring start positions at one phase
-    kLifetimePositionMajorDefer = 5,  // as 4, crossing computations deferred past the cheap tests
-    kLifetimePerThreadDefer = 6,      // as 2, crossing computations deferred past the cheap tests
-    kLifetimeVariants = 7
+    kLifetimePerThreadDefer = 6, // as 2, crossing computations deferred past the cheap tests (default)
 };
+
+inline bool lifetime_variant_known(int v)
+{
+    return v == kLifetimePerThread || v == kLifetimePerThreadLean || v == kLifetimePerThreadDefer;
+}
 
 constexpr int kIntegrateBlocks = 296;   // 2 x 148 SMs; fixed so the reduction order is fixed
 constexpr int kIntegrateThreads = 256;   // threads per block for 3+ temperatures; 1-2 temperatures use 512

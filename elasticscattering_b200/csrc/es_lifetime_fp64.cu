@@ -51,13 +51,10 @@ __device__ __forceinline__ void warp_flush(unsigned long long* metrics, unsigned
     }
 }
 
-// kPositionMajor = false: lanes take consecutive orbits of the storage order,
-// i.e. 32 phases of one start position. kPositionMajor = true: lanes take 32
-// neighbouring start positions of one row at the same phase; their orbits are
-// parallel shifts of each other (by the position spacing, a fraction of a
-// cell), so they cross the same cells and edges and scan the same impurity
-// lists, which keeps the warp converged. Stores are then strided.
-template <int kMinBlocks, bool kPositionMajor, int kDefer>
+// Lanes take consecutive orbits of the storage order, i.e. 32 phases of one
+// start position. kDefer > 0 parks crossing disks in shared memory and takes
+// their crossing points after the cheap tests of the cell (trace_orbit).
+template <int kMinBlocks, int kDefer>
 __global__ void __launch_bounds__(256, kMinBlocks) lifetime_fp64_kernel(LifetimeLaunch P)
 {
     __shared__ int s_defer[kDefer > 0 ? kDefer * kDeferStride : 1];
@@ -66,22 +63,11 @@ __global__ void __launch_bounds__(256, kMinBlocks) lifetime_fp64_kernel(Lifetime
     const unsigned mask = __ballot_sync(0xffffffffu, active);
     if (!active) return;
 
-    int v, i, j;
-    long long g;
-    if (kPositionMajor) {
-        // t = ((row * n_phase) + v) * dim + i over the rows of this launch
-        i = (int)(t % P.dim);
-        const long long rv = t / P.dim;
-        v = (int)(rv % P.n_phase);
-        j = P.row0 + (int)(rv / P.n_phase);
-        g = ((long long)j * P.dim + i) * P.n_phase + v;
-    } else {
-        g = (long long)P.row0 * P.dim * P.n_phase + t;
-        v = (int)(g % P.n_phase);
-        const long long pidx = g / P.n_phase;
-        i = (int)(pidx % P.dim);
-        j = (int)(pidx / P.dim);
-    }
+    const long long g = (long long)P.row0 * P.dim * P.n_phase + t;
+    const int v = (int)(g % P.n_phase);
+    const long long pidx = g / P.n_phase;
+    const int i = (int)(pidx % P.dim);
+    const int j = (int)(pidx / P.dim);
 
     // Simulation position grid, src/sim/SimulationCPU.cpp:114:
     // v2(i, j) * distance_between_positions + small_offset
@@ -128,207 +114,6 @@ __global__ void __launch_bounds__(256, kMinBlocks) lifetime_fp64_kernel(Lifetime
     if (P.out32) P.out32[g] = (float)lt;
 
     warp_flush(P.metrics, mask, cnt, flags, true);
-}
-
-// ---------------------------------------------------------------------------
-// Lane-refill variant: persistent warps. A lane owns one orbit at a time and
-// advances it one cell step per iteration; when its orbit finishes it takes the
-// next orbit of the warp's chunk, so a warp no longer idles while its longest
-// orbit walks on (orbits range from 0 to tens of cell steps). Warps take chunks
-// of kRefillChunk consecutive orbits from a global counter. Every orbit runs
-// exactly the reference's TraceOrbit sequence (trace_orbit in
-// es_orbit_fp64.cuh, unrolled into steps), so results are identical to the
-// one-thread-per-orbit kernel.
-constexpr int kRefillChunk = 128;
-
-struct LaneTally {
-    unsigned long long cells = 0, imps = 0, cross = 0, start = 0;
-    unsigned inside = 0, escaped = 0, bound = 0, max_cells = 0, max_imps = 0;
-};
-
-template <int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) lifetime_fp64_refill_kernel(LifetimeLaunch P)
-{
-    const unsigned kFull = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const unsigned lt_mask = (1u << lane) - 1u;
-
-    GridD gr;
-    gr.imps = P.imps;
-    gr.cell_end = P.cell_end;
-    gr.start = P.spawn_start;
-    gr.size = P.spawn_size;
-    gr.cell = P.cell_size;
-    gr.imp_r = P.imp_radius;
-    gr.cpr = P.cpr;
-
-    long long g = -1;  // orbit owned by this lane, -1 when idle
-    OrbitD o;
-    o.radius = P.radius;
-    o.radius_sq = P.radius_sq;
-    o.clockwise = P.clockwise != 0;
-    dv2 pos = {0.0, 0.0};
-    Isect next;
-    double lifetime = kINF;
-    int steps = 0, o_cells = 0, o_imps = 0;
-    bool started = false;
-    LaneTally tally;
-
-    long long chunk_next = 0, chunk_end = 0;  // warp-uniform
-    bool exhausted = false;                   // warp-uniform
-
-    for (;;) {
-        // ---- refill idle lanes from the warp's chunk ----
-        unsigned idle = __ballot_sync(kFull, g < 0);
-        while (idle != 0u && !exhausted) {
-            if (chunk_next >= chunk_end) {
-                unsigned long long base = 0;
-                if (lane == 0) base = atomicAdd(P.work, (unsigned long long)kRefillChunk);
-                base = __shfl_sync(kFull, base, 0);
-                if ((long long)base >= P.n_orbits) {
-                    exhausted = true;
-                    break;
-                }
-                chunk_next = (long long)base;
-                chunk_end = min((long long)base + kRefillChunk, P.n_orbits);
-            }
-            const long long avail = chunk_end - chunk_next;
-            const int r = __popc(idle & lt_mask);
-            if (g < 0 && r < avail) {
-                g = chunk_next + r;
-                // CreateParticle + TraceOrbit set-up (see lifetime_fp64_kernel)
-                const long long gg = (long long)P.row0 * P.dim * P.n_phase + g;
-                const int v = (int)(gg % P.n_phase);
-                const long long pidx = gg / P.n_phase;
-                const int i = (int)(pidx % P.dim);
-                const int j = (int)(pidx / P.dim);
-                pos = dv2{(double)i * P.dist + P.off_x, (double)j * P.dist + P.off_y};
-                const PhaseOrbit ph = P.phase[v];
-                const double shift_x = (ph.vel_y * P.radius) / P.speed;
-                const double shift_y = (-ph.vel_x * P.radius) / P.speed;
-                o.center = o.clockwise ? dv2{pos.x - shift_x, pos.y - shift_y} : dv2{pos.x + shift_x, pos.y + shift_y};
-                o.bound_time = P.coherent ? kINF : ph.bound_dphi / P.w;
-                o.particle_angle = ph.phi;
-                next.position = pos;
-                next.cell = get_cell(pos, gr.start, gr.size, gr.cpr);
-                next.dphi = kPI2;
-                next.incident_angle = ph.phi;
-                lifetime = kINF;
-                steps = o_cells = o_imps = 0;
-                started = false;
-            }
-            chunk_next += min((long long)__popc(idle), avail);
-            idle = __ballot_sync(kFull, g < 0);
-        }
-        if (__all_sync(kFull, g < 0)) break;
-        if (g < 0) continue;
-
-        // ---- one step of the owned orbit ----
-        int k0 = 0, k1 = 0;
-        bool avail_next = false;
-        double vr_x = 0.0, vr_y = 0.0;
-        bool finish = false;
-        double result = 0.0;
-        if (!started) {
-            if (!within_bounds(next.cell, gr.cpr)) {
-                atomicOr(P.error, kErrStartCell);
-                finish = true;
-            } else {
-                const int pci = next.cell.y * gr.cpr + next.cell.x;
-                k0 = (pci == 0) ? 0 : __ldg(gr.cell_end + pci - 1);
-                k1 = __ldg(gr.cell_end + pci);
-            }
-        } else {
-            Isect entry = next;
-            avail_next = next_cell(o, o.particle_angle, gr, entry, next);
-            vr_x = entry.incident_angle;
-            vr_y = avail_next ? next.incident_angle : o.particle_angle;
-            const int ci = entry.cell.y * gr.cpr + entry.cell.x;
-            k0 = (ci > 0) ? __ldg(gr.cell_end + ci - 1) : 0;
-            k1 = __ldg(gr.cell_end + ci);
-            o_cells += 1;
-            o_imps += k1 - k0;
-        }
-
-        bool inside = false;
-        for (int k = k0; k < k1; k++) {
-            const double2 imp = __ldg(gr.imps + k);
-            const dv2 ip = {imp.x, imp.y};
-            if (!started) {
-                tally.start += 1;
-                if (inside_impurity(pos, ip, gr.imp_r)) {
-                    inside = true;
-                    break;
-                }
-            } else if (circles_cross(o, ip, gr.imp_r)) {
-                tally.cross += 1;
-                const double t = first_cross_time(o, ip, gr.imp_r, P.w, vr_x, vr_y);
-                lifetime = (t < lifetime) ? t : lifetime;
-            }
-        }
-
-        if (!finish) {
-            if (!started) {
-                if (inside) {
-                    tally.inside += 1;
-                    finish = true;  // result 0
-                } else {
-                    started = true;
-                }
-            } else {
-                bool clamp = false;
-                if (lifetime < kINF) {
-                    finish = clamp = true;
-                    result = lifetime;
-                } else if (!avail_next) {
-                    tally.escaped += 1;
-                    finish = clamp = true;  // result 0, then the bound check
-                } else if (++steps >= P.walk_cap) {
-                    atomicOr(P.error, kErrWalkCap);
-                    finish = true;
-                }
-                if (clamp && result > o.bound_time) {
-                    tally.bound += 1;
-                    result = o.bound_time;
-                }
-            }
-        }
-        if (finish) {
-            P.out[(long long)P.row0 * P.dim * P.n_phase + g] = result;
-            if (P.out32) P.out32[(long long)P.row0 * P.dim * P.n_phase + g] = (float)result;
-            tally.cells += (unsigned)o_cells;
-            tally.imps += (unsigned)o_imps;
-            tally.max_cells = max(tally.max_cells, (unsigned)o_cells);
-            tally.max_imps = max(tally.max_imps, (unsigned)o_imps);
-            g = -1;
-        }
-    }
-
-    // ---- per-warp metric flush (all 32 lanes are here) ----
-    unsigned long long s_cells = tally.cells, s_imps = tally.imps, s_cross = tally.cross, s_start = tally.start;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        s_cells += __shfl_xor_sync(kFull, s_cells, off);
-        s_imps += __shfl_xor_sync(kFull, s_imps, off);
-        s_cross += __shfl_xor_sync(kFull, s_cross, off);
-        s_start += __shfl_xor_sync(kFull, s_start, off);
-    }
-    const unsigned s_inside = __reduce_add_sync(kFull, tally.inside);
-    const unsigned s_escaped = __reduce_add_sync(kFull, tally.escaped);
-    const unsigned s_bound = __reduce_add_sync(kFull, tally.bound);
-    const unsigned m_cells = __reduce_max_sync(kFull, tally.max_cells);
-    const unsigned m_imps = __reduce_max_sync(kFull, tally.max_imps);
-    if (lane == 0) {
-        if (s_cells) atomicAdd(P.metrics + kMetCells, s_cells);
-        if (s_imps) atomicAdd(P.metrics + kMetImps, s_imps);
-        if (s_cross) atomicAdd(P.metrics + kMetCrossings, s_cross);
-        if (s_start) atomicAdd(P.metrics + kMetStartTests, s_start);
-        if (s_inside) atomicAdd(P.metrics + kMetInside, (unsigned long long)s_inside);
-        if (s_escaped) atomicAdd(P.metrics + kMetEscaped, (unsigned long long)s_escaped);
-        if (s_bound) atomicAdd(P.metrics + kMetAtBound, (unsigned long long)s_bound);
-        if (m_cells) atomicMax(P.metrics + kMetMaxCells, (unsigned long long)m_cells);
-        if (m_imps) atomicMax(P.metrics + kMetMaxImps, (unsigned long long)m_imps);
-    }
 }
 
 __global__ void debug_next_cell_kernel(double cx, double cy, double r, int clockwise, double phi, double start,
@@ -404,31 +189,11 @@ cudaError_t launch_debug_trace(const LifetimeLaunch& L, const PhaseOrbit& ph, do
 
 namespace {
 
-template <int kMinBlocks>
-cudaError_t launch_refill(const LifetimeLaunch& L, cudaStream_t s)
-{
-    static int blocks_per_sm = 0, sms = 0;
-    if (blocks_per_sm == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, lifetime_fp64_refill_kernel<kMinBlocks>, 256, 0);
-        if (blocks_per_sm < 1) blocks_per_sm = 1;
-    }
-    cudaError_t e = cudaMemsetAsync(L.work, 0, sizeof(unsigned long long), s);
-    if (e != cudaSuccess) return e;
-    const long long warps_needed = (L.n_orbits + kRefillChunk - 1) / kRefillChunk;
-    long long blocks = (long long)sms * blocks_per_sm;
-    if (blocks * 8 > warps_needed) blocks = (warps_needed + 7) / 8;
-    lifetime_fp64_refill_kernel<kMinBlocks><<<(unsigned)blocks, 256, 0, s>>>(L);
-    return cudaGetLastError();
-}
-
-template <int kMinBlocks, bool kPositionMajor, int kDefer>
+template <int kMinBlocks, int kDefer>
 cudaError_t launch_per_thread(const LifetimeLaunch& L, cudaStream_t s)
 {
     const long long blocks = (L.n_orbits + 255) / 256;
-    lifetime_fp64_kernel<kMinBlocks, kPositionMajor, kDefer><<<(unsigned)blocks, 256, 0, s>>>(L);
+    lifetime_fp64_kernel<kMinBlocks, kDefer><<<(unsigned)blocks, 256, 0, s>>>(L);
     return cudaGetLastError();
 }
 
@@ -438,13 +203,9 @@ cudaError_t launch_lifetimes_fp64(const LifetimeLaunch& L, cudaStream_t s)
 {
     if (L.n_orbits <= 0) return cudaSuccess;
     switch (L.variant) {
-        case kLifetimePerThread: return launch_per_thread<3, false, 0>(L, s);
-        case kLifetimeRefill: return launch_refill<2>(L, s);
-        case kLifetimePerThreadLean: return launch_per_thread<4, false, 0>(L, s);
-        case kLifetimeRefillLean: return launch_refill<3>(L, s);
-        case kLifetimePositionMajor: return launch_per_thread<4, true, 0>(L, s);
-        case kLifetimePositionMajorDefer: return launch_per_thread<4, true, 4>(L, s);
-        case kLifetimePerThreadDefer: return launch_per_thread<4, false, 4>(L, s);
+        case kLifetimePerThread: return launch_per_thread<3, 0>(L, s);
+        case kLifetimePerThreadLean: return launch_per_thread<4, 0>(L, s);
+        case kLifetimePerThreadDefer: return launch_per_thread<4, 4>(L, s);
         default: return cudaErrorInvalidValue;
     }
 }

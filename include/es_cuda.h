@@ -102,8 +102,10 @@ typedef struct es_ctx es_ctx;
  * OpenCL launch shape is fixed, src/sim/SimulationCL.cpp:412-431); the
  * autotuner picks these, the defaults are the measured best on B200. */
 typedef struct es_tuning {
-    int32_t lifetime_variant;  /* 0 = one orbit per thread, 1 = persistent warps with lane refill,
-                                  2 / 3 = the same two with a tighter register budget */
+    int32_t lifetime_variant;  /* FP64 lifetime kernel: 0 = one orbit per thread (<= 80 registers),
+                                  2 = the same at <= 64 registers, 6 = as 2 with the crossing points of
+                                  a cell taken after its cheap tests (the default); other values are
+                                  rejected */
 } es_tuning;
 
 /* Replaces SimulationCL::SimulationCL (src/sim/SimulationCL.cpp:386-475): binds a
@@ -303,22 +305,20 @@ typedef struct es_batch_instance {
 /* How a batch maps its passes onto kernels. In every mode one graph replay
  * runs the whole batch; the autotuner picks the mode. */
 typedef enum es_batch_mode {
-    ES_BATCH_PASS_NODES = 0,  /* one kernel node per pass on parallel graph branches, the pass record
-                                 as kernel parameter; one block per 256 orbits */
-    ES_BATCH_GRID = 1,        /* one kernel over all passes, one block per 256 orbits, each block looks
-                                 its pass up in the device table */
+    /* values 0 and 1 named block-per-work-item modes that never won on B200 and were
+       removed; es_batch_set_tuning rejects them */
     ES_BATCH_PERSISTENT = 2,  /* one persistent kernel: warps take work items of 32 * chunk_iters
-                                 orbits of any pass from a global counter */
+                                 orbits of any pass from a global counter, stages (b)+(c) fused in */
     ES_BATCH_PASS_KERNELS = 3 /* the single-pass path's kernels for each pass in turn: the lifetime
                                  kernel (and, split, its FP64 re-trace) writes the pass's lifetimes
                                  to device scratch, the integration kernels reduce them to sigma;
-                                 chunk_iters and blocks_per_sm are not used */
+                                 chunk_iters and blocks_per_sm are not used (the default) */
 } es_batch_mode;
 
 /* Launch choices of a batch (picked by the autotuner). */
 typedef struct es_batch_tuning {
     int32_t chunk_iters;    /* ES_BATCH_PERSISTENT: orbits per work item = 32 * chunk_iters */
-    int32_t blocks_per_sm;  /* resident blocks of 256 threads per SM: 3 or 4 (register budget) */
+    int32_t blocks_per_sm;  /* ES_BATCH_PERSISTENT: resident blocks of 256 threads per SM, 3 or 4 */
     int32_t precision;      /* es_precision */
     int32_t mode;           /* es_batch_mode */
 } es_batch_tuning;

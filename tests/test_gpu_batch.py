@@ -141,12 +141,12 @@ def test_batch_bit_reproducible_and_shape_independent(sweep_inputs, cuda_device)
 
 
 def test_batch_modes_agree(sweep_inputs, cuda_device):
-    """Per-pass kernel nodes and the one-kernel grid cut the passes into the same
-    256-orbit blocks with the same reduction order: bit-identical. The persistent
-    kernel groups its sums differently: equal to rounding. Metrics are integers."""
+    """The persistent fused kernel and the per-pass kernels (the default) sum in
+    different orders: equal to rounding. Metrics are integers and equal. The
+    removed mode numbers are rejected."""
     ext, grids = sweep_inputs
     outs = {}
-    for mode in (N.ES_BATCH_PASS_NODES, N.ES_BATCH_GRID, N.ES_BATCH_PERSISTENT):
+    for mode in (N.ES_BATCH_PASS_KERNELS, N.ES_BATCH_PERSISTENT):
         b, ids = new_batch(grids, cuda_device, N.ES_PRECISION_SPLIT)
         try:
             b.set_tuning(mode=mode)
@@ -154,20 +154,29 @@ def test_batch_modes_agree(sweep_inputs, cuda_device):
             outs[mode] = b.run()
         finally:
             b.close()
-    (a, ma), (g, mg), (p, mp) = outs[N.ES_BATCH_PASS_NODES], outs[N.ES_BATCH_GRID], outs[N.ES_BATCH_PERSISTENT]
-    assert np.array_equal(a.view(np.int64), g.view(np.int64))
-    assert float(rel_err(p[:, :3], a[:, :3]).max()) <= FP64_RTOL
-    assert ma == mg == mp
+    (k, mk), (p, mp) = outs[N.ES_BATCH_PASS_KERNELS], outs[N.ES_BATCH_PERSISTENT]
+    assert float(rel_err(p[:, :3], k[:, :3]).max()) <= SPLIT_RTOL
+    for a, c in zip(mk, mp):
+        for key in ("cells_passed", "impurities_tested", "particles_inside_impurity", "particles_escaped",
+                    "particles_at_bound"):
+            assert a[key] == c[key], key
+    b, _ = new_batch(grids, cuda_device, N.ES_PRECISION_SPLIT)
+    try:
+        for mode in (0, 1, 4):
+            with pytest.raises(N.EsError):
+                b.set_tuning(mode=mode)
+    finally:
+        b.close()
 
 
 def test_batch_graph_replay_with_new_table(sweep_inputs, cuda_device):
     """The recorded graph is replayed with a rewritten instance table (same capacity
-    and work-item count; the one-kernel modes read the table from device memory)."""
+    and work-item count; the persistent kernel reads the table from device memory)."""
     ext, grids = sweep_inputs
     b, ids = new_batch(grids, cuda_device, N.ES_PRECISION_SPLIT)
     fresh, fids = new_batch(grids, cuda_device, N.ES_PRECISION_SPLIT)
-    b.set_tuning(mode=N.ES_BATCH_GRID)
-    fresh.set_tuning(mode=N.ES_BATCH_GRID)
+    b.set_tuning(mode=N.ES_BATCH_PERSISTENT)
+    fresh.set_tuning(mode=N.ES_BATCH_PERSISTENT)
     try:
         b.set_passes(make_passes(ext, grids, ids, fields=(1.5, 7.0)))
         b.run()

@@ -230,17 +230,21 @@ def test_lifetime_known_answers_on_device(cuda_device, golden):
 
 @pytest.mark.parametrize("coherent", [True, False])
 def test_lifetime_variants_agree_bitwise(config0_setup, coherent):
-    """The per-thread and lane-refill kernels schedule orbits differently but run
-    the same arithmetic: lifetimes and every metric counter are identical."""
+    """The FP64 kernel's register budgets and its deferred crossing form run the
+    same arithmetic: lifetimes and every metric counter are identical. Removed
+    variant numbers are rejected."""
     w, g, og, sim = config0_setup
     sim.InitSample(g, settings_of(w), coherent)
     default = sim.get_tuning()
     runs = {}
-    for variant in range(7):
+    for variant in (0, 2, 6):
         sim.set_tuning(lifetime_variant=variant)
         runs[variant] = sim.ComputeLifetimes(5.0)
+    for variant in (1, 3, 4, 5, 7, -1):
+        with pytest.raises(EsError):
+            sim.set_tuning(lifetime_variant=variant)
     sim.set_tuning(**default)
-    for variant in range(1, 7):
+    for variant in (2, 6):
         assert np.array_equal(runs[0][0].view(np.int64), runs[variant][0].view(np.int64)), variant
         assert runs[0][1] == runs[variant][1], variant
 
