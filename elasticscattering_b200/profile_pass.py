@@ -2,6 +2,7 @@
 
     python -m elasticscattering_b200.profile_pass --workload config1 --field 20 --coherent 0 [--passes 1]
         [--variant V] [--time]
+    python -m elasticscattering_b200.profile_pass --slice [--passes K]
 
 Builds the workload's impurity field on the host, uploads it, and runs
 `--passes` lifetime passes (stage a) followed by one integration (stages b, c),
@@ -35,13 +36,20 @@ def main() -> None:
     ap.add_argument("--batch", action="store_true",
                     help="run the pass through the batched kernel (one instance, fused integration)")
     ap.add_argument("--mode", type=int, default=N.ES_BATCH_PERSISTENT,
-                    help="--batch: es_batch_mode (0 pass nodes, 1 grid, 2 persistent, 3 single-pass kernels)")
+                    help="--batch: es_batch_mode (2 persistent, 3 single-pass kernels)")
+    ap.add_argument("--slice", action="store_true",
+                    help="the bench's step: the representative 3-sample slice of the 64-sample, 32-field sweep "
+                         "(one 129^2, 257^2 and 513^2 sample; 192 passes) in one graph replay of the default "
+                         "batch mode, --passes replays")
     ap.add_argument("--chunk-iters", type=int, default=32)
     ap.add_argument("--sweep-sample", type=int, default=None,
                     help="--batch: run sample K of the 64-sample batched sweep draw instead of --workload")
     ap.add_argument("--sweep-fields", type=int, default=2, help="--sweep-sample: fields uniformly spaced 1-40 T")
     ap.add_argument("--tcp", type=int, default=12, help="--sweep-sample: target cell population")
     a = ap.parse_args()
+    if a.slice:
+        batch_slice(a)
+        return
     if a.compare_split:
         compare_split(a)
         return
@@ -150,6 +158,34 @@ def batch_sweep_sample(a) -> None:
                       "tcp": a.tcp, "fields": wl.fields, "orbits": orbits, "ms": ms,
                       "retraced_fp64": sum(x["retraced_fp64"] for x in m),
                       "impurities_tested": sum(x["impurities_tested"] for x in m),
+                      "cells_passed": sum(x["cells_passed"] for x in m)}))
+
+
+def batch_slice(a) -> None:
+    """The bench's step (bench.py's default workload) with the library's default
+    batch tuning and the reference's cell population: graph replays of the
+    representative slice, each timed with CUDA events on the batch stream."""
+    from .batch import BatchSweep, sweep_passes
+    wl = workloads.representative_slice(workloads.config2(), 0)
+    grids = {s.index: Grid.from_seed(s.seed, wl.region_size, wl.region_extends, s.density, wl.impurity_radius,
+                                     wl.target_cell_population) for s in wl.samples}
+    prec = N.ES_PRECISION_SPLIT if a.precision is None else a.precision
+    with BatchSweep(precision=prec) as b:
+        ids = {k: b.add_grid(g) for k, g in grids.items()}
+        b.set_passes(sweep_passes(wl, ids, {k: g.info().cell_size for k, g in grids.items()}))
+        import torch
+        stream = torch.cuda.ExternalStream(b.stream_handle())
+        ms = []
+        for _ in range(a.passes):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.enqueue()
+            e1.record(stream)
+            out, m = b.collect()
+            ms.append(round(e0.elapsed_time(e1), 3))
+        orbits = b.total_orbits
+    print(json.dumps({"workload": wl.name, "orbits": orbits, "passes": len(m), "ms": ms,
+                      "retraced_fp64": sum(x["retraced_fp64"] for x in m),
                       "cells_passed": sum(x["cells_passed"] for x in m)}))
 
 
