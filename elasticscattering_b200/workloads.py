@@ -181,18 +181,34 @@ def shard_samples(wl: BatchWorkload, rank: int, world: int, per_rank: int) -> Ba
 
 
 def representative_slice(wl: BatchWorkload, k: int = 0) -> BatchWorkload:
-    """Three samples of the draw, one per start grid -- the k-th 129^2, the k-th
-    257^2 and the k-th 513^2 sample -- with every field and temperature. The
-    draw picks each start grid with probability 1/3, so this slice holds the
-    orbits of three average samples; slices k = 0, 1, ... are disjoint (the
-    per-GPU work of a weak-scaling run)."""
+    """Three samples of the draw, one per start grid (129^2, 257^2, 513^2), with
+    every field and temperature: the draw picks each start grid with probability
+    1/3, so the slice holds the orbits of three average samples. The samples are
+    matched greedily so that the slice's estimated cost per orbit (sample_cost)
+    is as close as possible to the whole draw's: slice 0 takes the best triple,
+    slice 1 the best of the remaining samples, and so on, so slices k = 0, 1, ...
+    are disjoint (the per-GPU work of a weak-scaling run) and each times like
+    the sweep it stands for."""
     import copy
-    picked = []
-    for d in sorted({s.dim for s in wl.samples}):
-        of_dim = [s for s in wl.samples if s.dim == d]
-        if k >= len(of_dim):
-            raise ValueError(f"the draw holds {len(of_dim)} samples of {d}^2 start positions; slice {k} requested")
-        picked.append(of_dim[k])
+    import itertools
+    dims = sorted({s.dim for s in wl.samples})
+    by_dim = {d: [s for s in wl.samples if s.dim == d] for d in dims}
+    cost = {s.index: sample_cost(wl, s) for s in wl.samples}
+    per_pass = 4 * wl.phi_steps * 2 * len(wl.fields)
+    target = sum(cost.values()) / (sum(s.dim * s.dim for s in wl.samples) * per_pass)
+    used: set = set()
+    picked = None
+    for _ in range(k + 1):
+        best, best_key = None, None
+        for trio in itertools.product(*[[s for s in by_dim[d] if s.index not in used] for d in dims]):
+            cpo = sum(cost[s.index] for s in trio) / (sum(s.dim * s.dim for s in trio) * per_pass)
+            key = (abs(cpo - target), [s.index for s in trio])
+            if best_key is None or key < best_key:
+                best, best_key = trio, key
+        if best is None:
+            raise ValueError(f"the draw holds too few samples of each start grid for slice {k}")
+        used |= {s.index for s in best}
+        picked = list(best)
     out = copy.copy(wl)
     out.samples = picked
     out.name = f"{wl.name.split('-')[0]}-slice{k}-{len(picked)}x{len(wl.fields)}x{len(wl.temperatures)}"

@@ -92,10 +92,18 @@ def test_sample_cost_grows_with_orbits_and_density():
 
 def test_representative_slices_are_disjoint_with_one_sample_per_start_grid():
     wl = workloads.config2()
+    per_pass = 4 * wl.phi_steps * 2 * len(wl.fields)
+
+    def cost_per_orbit(samples):
+        return sum(workloads.sample_cost(wl, s) for s in samples) / (sum(s.dim ** 2 for s in samples) * per_pass)
+
+    target = cost_per_orbit(wl.samples)
     seen = set()
     for k in range(8):
         sl = workloads.representative_slice(wl, k)
         assert sorted(s.dim for s in sl.samples) == [129, 257, 513]
+        # each slice's estimated cost per orbit stands for the whole draw's
+        assert abs(cost_per_orbit(sl.samples) - target) <= 0.07 * target, k
         idx = {s.index for s in sl.samples}
         assert not (idx & seen)
         seen |= idx
