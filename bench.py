@@ -633,7 +633,7 @@ def integrate_roofline(wl, s, tcp_for, dev, flush, torch, N) -> dict:
         out[name] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": src, "avg_launch_ms": per[1], "ms_at_all_temperatures": per[len(temps)],
                      "temperatures_at_once": len(temps),
-                     "traffic": profiled_traffic(f"integrate_flat_{name}_config2.md", n),
+                     "traffic": profiled_traffic(f"integrate_flat_{name}_config1.md", n),
                      "kernel": "integrate_flat_kernel + reduce_partials_kernel",
                      "work": f"{bytes_alg:.4g} algorithmic bytes per launch (8-byte lifetimes of one "
                              f"{s.dim}^2 x {4 * wl.phi_steps}-orbit pass, one temperature)"}

@@ -1085,6 +1085,7 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
         L.coherent = x.coherent ? 1 : 0;
         L.walk_cap = H::walk_cap_for(L.radius, L.cell_size);
         L.imps32 = g.d_imps32;
+        H::split_constants(L);
         d.phase_sigma = p.d_sigma;
         d.acc = b->d_acc + (size_t)pos * 2 * es::kBatchMaxTau;
         d.metrics = b->d_metrics + (size_t)pos * es::kMetCount;

@@ -163,6 +163,7 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.retrace_count = ctx->d_retrace_count;
     L.retrace_cap = ctx->retrace_cap;
     L.orbit_table = ctx->d_orbit_table;
+    es::host::split_constants(L);
     return L;
 }
 

@@ -78,6 +78,25 @@ inline int walk_cap_for(double radius, double cell)
     return steps > 2.0e9 ? 2000000000 : (int)steps;
 }
 
+// The split walk's FP32 constants of a pass (trace_split in es_orbit_split.cuh
+// uses them; they depend on the orbit radius, the impurity radius and the cell
+// size only). The same IEEE operations as the device expressions they replace:
+// FP64 products rounded to FP32 once, FP32 products rounded after each step.
+inline void split_constants(LifetimeLaunch& L)
+{
+    const double r64 = L.radius, ir64 = L.imp_radius;
+    L.sc_r = (float)r64;
+    L.sc_inv_r = (float)(1.0 / r64);
+    L.sc_ir = (float)ir64;
+    L.sc_lo2 = (float)((r64 - ir64) * (r64 - ir64));
+    L.sc_hi2 = (float)((r64 + ir64) * (r64 + ir64));
+    const float t = 2e-6f * L.sc_r;
+    L.sc_eps2 = t * L.sc_r;
+    L.sc_band_d = 0.02f * L.sc_ir;
+    L.sc_inv4r = 0.25f * L.sc_inv_r;
+    L.sc_tangent_tol = (float)((0.01 * L.cell_size * L.cell_size) * (double)L.sc_inv_r + 2e-7 * L.cell_size);
+}
+
 // Sector constants of Simulation::InitSample (src/sim/Simulation.h:111-126).
 struct Sector {
     double area, phi_integrand_factor, phi_start, phi_step;

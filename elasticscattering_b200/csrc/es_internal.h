@@ -69,6 +69,10 @@ struct LifetimeLaunch {
     // radius and w, written by orbit_table_kernel before the lifetime kernel
     // (null: computed per orbit).
     double4* orbit_table;
+    // The split walk's FP32 constants of this pass (split_constants in
+    // es_host_math.h): as kernel parameters they are constant-bank operands
+    // instead of registers.
+    float sc_r, sc_inv_r, sc_ir, sc_lo2, sc_hi2, sc_eps2, sc_band_d, sc_inv4r, sc_tangent_tol;
 };
 
 // FP64 lifetime kernel choices (es_tuning.lifetime_variant). The values 1, 3,

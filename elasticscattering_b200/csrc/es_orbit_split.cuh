@@ -74,6 +74,16 @@ struct LaunchFields {
     __device__ __forceinline__ int coherent() const { return P.coherent; }
     __device__ __forceinline__ int walk_cap() const { return P.walk_cap; }
     __device__ __forceinline__ const double4* orbit_table() const { return P.orbit_table; }
+    // the pass's FP32 walk constants, host-computed launch parameters
+    __device__ __forceinline__ float r32() const { return P.sc_r; }
+    __device__ __forceinline__ float inv_r32() const { return P.sc_inv_r; }
+    __device__ __forceinline__ float ir32() const { return P.sc_ir; }
+    __device__ __forceinline__ float lo2() const { return P.sc_lo2; }
+    __device__ __forceinline__ float hi2() const { return P.sc_hi2; }
+    __device__ __forceinline__ float eps2() const { return P.sc_eps2; }
+    __device__ __forceinline__ float band_d() const { return P.sc_band_d; }
+    __device__ __forceinline__ float inv4r() const { return P.sc_inv4r; }
+    __device__ __forceinline__ float tangent_tol() const { return P.sc_tangent_tol; }
 };
 
 struct SharedFields {
@@ -104,6 +114,15 @@ struct SharedFields {
     __device__ __forceinline__ int coherent() const { return P->coherent; }
     __device__ __forceinline__ int walk_cap() const { return P->walk_cap; }
     __device__ __forceinline__ const double4* orbit_table() const { return nullptr; }
+    __device__ __forceinline__ float r32() const { return P->sc_r; }
+    __device__ __forceinline__ float inv_r32() const { return P->sc_inv_r; }
+    __device__ __forceinline__ float ir32() const { return P->sc_ir; }
+    __device__ __forceinline__ float lo2() const { return P->sc_lo2; }
+    __device__ __forceinline__ float hi2() const { return P->sc_hi2; }
+    __device__ __forceinline__ float eps2() const { return P->sc_eps2; }
+    __device__ __forceinline__ float band_d() const { return P->sc_band_d; }
+    __device__ __forceinline__ float inv4r() const { return P->sc_inv4r; }
+    __device__ __forceinline__ float tangent_tol() const { return P->sc_tangent_tol; }
 };
 
 __device__ __forceinline__ float wrap2pi(float a) { return a - kTwoPiF * floorf(a * (1.0f / kTwoPiF)); }
@@ -277,17 +296,19 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
                                            double& out, int2& win)
 {
     const double r64 = o.radius;
-    const double ir64 = f.imp_radius();
-    const float r = (float)r64;
-    const float inv_r = (float)(1.0 / r64);
-    const float ir = (float)ir64;
+    // The pass's FP32 constants (split_constants, es_host_math.h): r, 1/r, r_i;
     // CirclesCross in d^2: anything outside [lo2 - eps2, hi2 + eps2] misses for
-    // sure (the FP32 d^2 error is below 3e-7 r^2); inside, |d - r| decides, and
-    // within band_d of the edge the decision and the angle are taken in FP64.
-    const float lo2 = (float)((r64 - ir64) * (r64 - ir64)), hi2 = (float)((r64 + ir64) * (r64 + ir64));
-    const float eps2 = 2e-6f * r * r;
-    const float band_d = 0.02f * ir;
-    const float inv4r = 0.25f * inv_r;
+    // sure (the FP32 d^2 error is below 3e-7 r^2), where lo2 = (r - r_i)^2 and
+    // hi2 = (r + r_i)^2 in FP64 rounded once, eps2 = 2e-6 r^2; inside, |d - r|
+    // decides, and within band_d = 0.02 r_i of the edge the decision and the
+    // angle are taken in FP64; inv4r = 1 / (4 r).
+    const float r = f.r32();
+    const float inv_r = f.inv_r32();
+    const float ir = f.ir32();
+    const float lo2 = f.lo2(), hi2 = f.hi2();
+    const float eps2 = f.eps2();
+    const float band_d = f.band_d();
+    const float inv4r = f.inv4r();
     // Position angle of the start: C = pos -/+ r (sin phi, -cos phi) (details.h:243-250).
     const float dir = o.clockwise ? -1.0f : 1.0f;
     const float psi0 = (float)(o.clockwise ? o.particle_angle - kHALF_PI : o.particle_angle + kHALF_PI);
@@ -342,7 +363,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
     // at such a point has r - |c| <= r (0.1 L / r)^2 + 2e-7 L = tangent_tol.
     float la[4], lb[4];
     unsigned tangent = 0;
-    const float tangent_tol = (float)((0.01 * f.cell_size() * f.cell_size()) * (double)inv_r + 2e-7 * f.cell_size());
+    const float tangent_tol = f.tangent_tol();  // r (0.1 L / r)^2 + 2e-7 L
     {
         const double L = f.cell_size();
         const double llx0 = f.spawn_start() + cx * L, lly0 = f.spawn_start() + cy * L;

@@ -64,3 +64,14 @@ def test_reference_arm_default_is_the_config2_slice():
     assert d["config"]["workload"] == "config2-slice0-3x32x3"
     assert d["value"] > 0 and d["sigma_points_per_sec"] > 0
     assert d["e2e"]["value"] == d["value"]
+
+
+def test_integrate_traffic_comes_from_the_committed_profiles():
+    """The bench's stages-(b)+(c) roofline reads its DRAM traffic from the committed ncu
+    summaries of integrate_flat_kernel: about the 8 algorithmic bytes per orbit."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    for name in ("split", "fp64"):
+        n = 135_797_636  # a 513^2 x 516 pass
+        t = bench.profiled_traffic(f"integrate_flat_{name}_config1.md", n)
+        assert t is not None and 8 * n <= t <= 1.05 * 8 * n, (name, t)

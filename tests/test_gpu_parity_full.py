@@ -94,6 +94,7 @@ def compare(gpu: np.ndarray, ref: np.ndarray, phase_bound: np.ndarray | None) ->
 
 def check_pass(tag, gpu_lt, gpu_m, gpu_sig, res, precision, phase_bound, temps=TEMPS):
     r = compare(gpu_lt, res.lifetimes(), phase_bound)
+    print("pass", tag, r)  # the per-orbit figures behind the module docstring (pytest -s)
     assert r["flips"] == 0, (tag, r)
     if gpu_sig is not None:
         tol = SIGMA_RTOL[precision]
@@ -193,6 +194,7 @@ def test_config3_full_size_row_bands(cuda_device, ref_pool):
                 for band, res in zip(bands, refs):
                     lt = sim.ReadLifetimes(band[0] * per_row, (band[1] - band[0]) * per_row)
                     r = compare(lt, res.lifetimes(), pb)
+                    print("band", (coh, precision, band), r)
                     assert r["flips"] == 0 and r["max_rel"] <= LIFETIME_RTOL, (coh, precision, band, r)
         ref_pool.discard(refs)
 
