@@ -178,7 +178,7 @@ def tune_sweep(wl, device: int = 0, n_classes: int = 3, cache: Path | None = Non
     store[key] = asdict(res)
     try:
         cache.parent.mkdir(parents=True, exist_ok=True)
-        tmp = cache.with_suffix(".tmp")
+        tmp = cache.with_suffix(f".{os.getpid()}.tmp")  # ranks of a multi-GPU run tune at once
         tmp.write_text(json.dumps(store, indent=1))
         tmp.replace(cache)
     except OSError:
