@@ -934,8 +934,8 @@ def run_batched(args) -> None:
                      "kernel": "lifetime_split_kernel + lifetime_retrace_kernel (per pass, in the graph)",
                      "work": "algorithmic FP64-op count of the reference's TraceOrbit (flop_model) over the "
                              "graph replay, divided by the replay's device time (the lifetime kernels are "
-                             "~99% of it); traffic is per average pass",
-                     "flop_model": FLOP_MODEL},
+                             "~98% of it); traffic is per average pass",
+                     "flop_model": FLOP_MODEL, "issue": profiled_issue("split")},
         "roofline_integrate": integ,
         "split_vs_fp64": {"results": int(rel.size), "max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
                           "above_1e-6": int((rel > 1e-6).sum()), "sigma_points_max_rel": float(prel.max()),
