@@ -205,9 +205,12 @@ class Simulator:
         self.device = device
         self.levels = np.exp(np.linspace(math.log(N_RANGE[0]), math.log(N_RANGE[1]), self.res.density_levels))
         self.grids = {}
-        # thousands of small passes per call: the one persistent kernel, which
-        # has no per-pass launches (the per-pass-kernels default suits large passes)
-        self.batch = BatchSweep(device, mode=N.ES_BATCH_PERSISTENT)
+        # Thousands of small passes per call take the one persistent kernel, which
+        # has no per-pass launches; passes of a million orbits and up (129^2 start
+        # positions and more) take the per-pass kernels, the faster mode there.
+        orbits = self.res.dim * self.res.dim * 4 * self.res.phi_steps
+        mode = N.ES_BATCH_PASS_KERNELS if orbits >= (1 << 20) else N.ES_BATCH_PERSISTENT
+        self.batch = BatchSweep(device, mode=mode)
         self.grid_ids = {}
 
     def close(self) -> None:
