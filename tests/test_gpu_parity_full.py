@@ -17,9 +17,10 @@ plain FP64 path and within 1e-6 on the FP32/FP64 split path, and the
 reference's metric counters equal. Per-orbit lifetimes are held to 1e-6
 relative: the one libm call on the device path, asin in GetAngle, differs from
 glibc's in the last bit, and near tangency (a crossing point where the orbit
-barely enters a disk) that difference is amplified -- up to 1.6e-7 measured on
-these passes, where 88% of the lifetimes are bit-identical. (Compiling the
-reference itself with FMA contraction moves its own lifetimes by up to 5.3e-8.)
+barely enters a disk) that difference is amplified -- up to 2.3e-7 measured over
+the 47 passes and bands compared here, where 88-98% of the lifetimes are
+bit-identical. (Compiling the reference itself with FMA contraction moves its own
+lifetimes by up to 5.3e-8.)
 The split path's lifetimes are the plain GPU path's, bit for bit.
 """
 from __future__ import annotations
