@@ -479,7 +479,10 @@ struct es_batch {
     // slot per distinct tau) and the scratch the single-pass kernels share
     double* d_psigma = nullptr;
     double* h_psigma = nullptr;                // pinned
-    double* d_lt = nullptr;                    // one pass's lifetimes
+    // three passes' lifetimes in rotation: pass p writes d_lt[p % 3] and, split,
+    // reads the lifetimes of the pass one or two before it over the same orbits
+    // (another field) as its walk-length prediction
+    double* d_lt[3] = {};
     long long lt_cap = 0;
     double4* d_otab = nullptr;                 // one pass's orbit table (split)
     long long otab_cap = 0;
@@ -542,10 +545,12 @@ void free_tables(es_batch* b)
 
 void free_pass_scratch(es_batch* b)
 {
-    cudaFree(b->d_lt);
+    for (double*& p : b->d_lt) {
+        cudaFree(p);
+        p = nullptr;
+    }
     cudaFree(b->d_otab);
     cudaFree(b->d_partial);
-    b->d_lt = nullptr;
     b->d_otab = nullptr;
     b->d_partial = nullptr;
     b->lt_cap = b->otab_cap = 0;
@@ -614,7 +619,7 @@ es_status ensure_pass_scratch(es_batch* b)
     if (max_orbits <= b->lt_cap && max_phase <= b->otab_cap && b->d_partial) return ES_OK;
     drop_graph(b);
     free_pass_scratch(b);
-    ES_BCUDA(cudaMalloc(&b->d_lt, sizeof(double) * (size_t)max_orbits), "pass lifetimes");
+    for (double*& p : b->d_lt) ES_BCUDA(cudaMalloc(&p, sizeof(double) * (size_t)max_orbits), "pass lifetimes");
     ES_BCUDA(cudaMalloc(&b->d_otab, sizeof(double4) * (size_t)max_phase), "pass orbit table");
     ES_BCUDA(cudaMalloc(&b->d_partial, sizeof(double) * 2 * es::kMaxTChunk * es::kIntegrateBlocks),
              "integration partials");
@@ -636,8 +641,25 @@ cudaError_t record_pass_kernels(es_batch* b)
         const int k = b->order[pos];
         const es_batch_grid& g = b->grids[(size_t)b->inst[(size_t)k].grid];
         es::LifetimeLaunch L = d.L;
-        L.out = b->d_lt;
+        L.out = b->d_lt[pos % 3];
         L.out32 = nullptr;
+        L.pred = nullptr;
+        if (b->tuning.precision == ES_PRECISION_SPLIT) {
+            // the nearest of the two passes before this one over the same orbits
+            const es_batch_instance& x = b->inst[(size_t)k];
+            for (size_t q = pos; q-- > 0 && q + 2 >= pos;) {
+                const es_batch_instance& y = b->inst[(size_t)b->order[q]];
+                if (y.grid == x.grid && y.positions_per_row == x.positions_per_row &&
+                    y.particles_per_quadrant == x.particles_per_quadrant && y.coherent == x.coherent &&
+                    y.region_size == x.region_size && y.grid_cell_size == x.grid_cell_size &&
+                    y.settings.alpha == x.settings.alpha && y.settings.is_clockwise == x.settings.is_clockwise &&
+                    y.settings.particle_speed == x.settings.particle_speed) {
+                    L.pred = b->d_lt[q % 3];
+                    L.pred_scale = x.settings.particle_speed / g.is.cell_size;
+                    break;
+                }
+            }
+        }
         L.metrics = d.metrics;
         L.row0 = 0;
         L.variant = es::kLifetimePerThreadDefer;
@@ -653,7 +675,7 @@ cudaError_t record_pass_kernels(es_batch* b)
             e = es::launch_lifetimes_fp64(L, b->stream);
         if (e != cudaSuccess) break;
         es::IntegrateLaunch I{};
-        I.lifetimes = b->d_lt;
+        I.lifetimes = b->d_lt[pos % 3];
         I.phase = d.phase_sigma;
         for (int u = 0; u < d.n_tau; u++) {
             I.tau[u] = d.tau[u];

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <utility>
 #include <vector>
 
 namespace {
@@ -54,6 +55,11 @@ struct es_ctx {
     int n_phase = 0;
     int n_pos = 0;
     double* d_lifetimes = nullptr;
+    // split precision: the previous pass's lifetimes (same grid, sector and rows,
+    // another field), the walk-length prediction of the next pass; the two
+    // buffers swap roles every pass
+    double* d_prev = nullptr;
+    bool prev_valid = false;
     es::PhaseOrbit* d_phase_orbit = nullptr;
     double4* d_orbit_table = nullptr;  // split precision: the pass's per-phase orbit table
     es::PhaseSigma* d_phase_sigma = nullptr;
@@ -164,6 +170,8 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.retrace_cap = ctx->retrace_cap;
     L.orbit_table = ctx->d_orbit_table;
     es::host::split_constants(L);
+    L.pred = nullptr;
+    L.pred_scale = speed / ctx->is.cell_size;
     return L;
 }
 
@@ -177,8 +185,16 @@ es_status enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
     if (ctx->desc.precision == ES_PRECISION_SPLIT) {
         const bool defer = es::host::long_walks(ctx->n_imps, ctx->is.cells_per_row, ctx->is.cell_size,
                                                 ctx->is.impurity_radius);
-        ES_CUDA(es::launch_lifetimes_split(L, defer, ctx->stream), "split lifetime kernel launch");
+        es::LifetimeLaunch Ls = L;
+        if (ctx->prev_valid && ctx->d_prev) {
+            // this pass writes the other buffer and reads the last pass's lifetimes
+            std::swap(ctx->d_lifetimes, ctx->d_prev);
+            Ls.out = ctx->d_lifetimes;
+            Ls.pred = ctx->d_prev;
+        }
+        ES_CUDA(es::launch_lifetimes_split(Ls, defer, ctx->stream), "split lifetime kernel launch");
         ctx->launches += 3;  // orbit table, lifetime walk, FP64 re-trace
+        ctx->prev_valid = ctx->d_prev != nullptr;
     } else {
         ES_CUDA(es::launch_lifetimes_fp64(L, ctx->stream), "lifetime kernel launch");
         ctx->launches++;
@@ -302,6 +318,7 @@ void release(es_ctx* ctx)
     cudaFree(ctx->d_imps);
     cudaFree(ctx->d_cell_end);
     cudaFree(ctx->d_lifetimes);
+    cudaFree(ctx->d_prev);
     cudaFree(ctx->d_phase_orbit);
     cudaFree(ctx->d_orbit_table);
     cudaFree(ctx->d_phase_sigma);
@@ -371,6 +388,8 @@ es_status es_create(const es_sim_desc* desc, es_ctx** out)
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_phase_orbit, sizeof(es::PhaseOrbit) * n_phase);
     if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT)
         e = cudaMalloc(&ctx->d_orbit_table, sizeof(double4) * n_phase);
+    if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT)
+        e = cudaMalloc(&ctx->d_prev, sizeof(double) * ctx->n_orbits);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_phase_sigma, sizeof(es::PhaseSigma) * n_phase);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_metrics, sizeof(unsigned long long) * es::kMetCount);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(int));
@@ -453,6 +472,7 @@ es_status upload_arrays(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, co
     ctx->generation = generation;
     ctx->has_grid = true;
     ctx->lifetimes_valid = false;
+    ctx->prev_valid = false;
     return ES_OK;
 }
 
@@ -485,6 +505,7 @@ es_status es_set_rows(es_ctx* ctx, int32_t j0, int32_t j1)
     ctx->row0 = j0;
     ctx->row1 = j1;
     ctx->lifetimes_valid = false;
+    ctx->prev_valid = false;
     return ES_OK;
 }
 
@@ -584,6 +605,7 @@ es_status es_init_sample(es_ctx* ctx, const es_settings* s, int32_t coherent)
     ES_CUDA(cudaStreamSynchronize(ctx->stream), "phase table upload");
     ctx->has_sample = true;
     ctx->lifetimes_valid = false;
+    ctx->prev_valid = false;
     return ES_OK;
 }
 
