@@ -180,9 +180,13 @@ class MLPEnsemble:
 
 @dataclass
 class Resolution:
-    """Simulator resolution used for training data and fallback answers."""
-    dim: int = 65
-    phi_steps: int = 25
+    """Simulator resolution used for training data, fallback answers and judging:
+    by default the batched sweep's (config-2) resolution, 129^2 start positions x
+    516 phases. (At 65^2 x 100 the simulator's sigma differs from this resolution's
+    by p95 82 %: the phase and position integrals of a discontinuous integrand
+    converge slowly, so a network trained there learns the wrong function.)"""
+    dim: int = 129
+    phi_steps: int = 129
     region_size: float = 1e-6
     b_min: float = B_RANGE[0]     # sets region_extends (one orbit diameter at b_min)
     density_levels: int = 16      # densities are snapped to this many log-spaced levels
@@ -295,6 +299,34 @@ def sample_queries(n: int, seed: int, b_range=B_RANGE, n_range=N_RANGE, tau_rang
     q[:, 3] = radius
     q[:, 4] = logu(*tau_range, n)
     return q
+
+
+# Sub-ranges where the network's error concentrated (low field, long tau, low T):
+# training_queries draws part of the set there, still inside the config-4 ranges.
+HARD_B = (0.5, 2.0)
+HARD_TAU = (3e-12, 1e-11)
+HARD_T = (0.0, 5.0)
+
+
+def training_queries(n: int, seed: int, hard_fraction: float = 0.5, radius: float = R_SCALE) -> np.ndarray:
+    """The training draw: (1 - hard_fraction) of the rows as sample_queries over
+    the full config-4 ranges; the rest the same draw with one coordinate, in
+    turn, redrawn log-uniformly (T uniformly) over its hard sub-range."""
+    nh = int(round(n * hard_fraction))
+    base = sample_queries(n - nh, seed, radius=radius)
+    if nh == 0:
+        return base
+    hard = sample_queries(nh, seed + 1, radius=radius)
+    rng = np.random.default_rng(seed + 2)
+    k = rng.integers(0, 3, nh)
+
+    def logu(lo, hi, size):
+        return np.exp(rng.uniform(math.log(lo), math.log(hi), size))
+
+    hard[k == 0, 0] = logu(*HARD_B, int((k == 0).sum()))
+    hard[k == 1, 4] = logu(*HARD_TAU, int((k == 1).sum()))
+    hard[k == 2, 1] = rng.uniform(*HARD_T, int((k == 2).sum()))
+    return np.concatenate([base, hard])
 
 
 class Surrogate:

@@ -102,37 +102,40 @@ def test_training_fits_and_is_reproducible(cuda_device):
 
 
 def test_surrogate_answers_within_tolerance_or_falls_back(cuda_device):
-    """Reduced physics range (B 4-40 T, density 5e14-3e15 m^-2; the simulator at
-    65^2 starts x 100 phases): 4000 simulator queries train the ensemble; on 200
-    held-out queries the network answers where its members agree to 1% -- those
-    answers are within 1% of the simulator (95th percentile; 3% at most) -- the
-    rest fall back to the simulator, and the network answers a batch far faster
-    than the simulator does."""
-    res = S.Resolution(dim=65, phi_steps=25, b_min=4.0, density_levels=6)
-    sim = S.Simulator(res, device=cuda_device)
+    """The full config-4 ranges (B 0.5-50 T, density 5e14-2e16 m^-2, tau 1e-13-1e-11 s,
+    T 0-40 K) with the simulator at the batched sweep's resolution (129^2 starts x 516
+    phases): 20k simulator runs train the ensemble on the GPU; on 512 held-out
+    queries of the config-4 draw the network answers where its members agree to 1 %
+    (the stated fallback tolerance) -- those answers are within 1 % of the simulator
+    at the 95th percentile (3 % at most) -- the rest fall back to the simulator, and
+    the network answers a batch at least 100x faster than the simulator does."""
+    sim = S.Simulator(S.Resolution(), device=cuda_device)
     try:
-        kw = dict(b_range=(4.0, 40.0), n_range=(5e14, 3e15))
-        sim.levels = np.exp(np.linspace(np.log(5e14), np.log(3e15), res.density_levels))
-        train_q = sim.snapped(S.sample_queries(4000, seed=1, **kw))
+        sim.prebuild(sim.levels)
+        train_q = sim.snapped(S.training_queries(20000, seed=1))
         train_s = sim(train_q)
-        test_q = sim.snapped(S.sample_queries(200, seed=2, **kw))
+        test_q = sim.snapped(S.sample_queries(512, seed=2))
         t0 = time.perf_counter()
         truth = sim(test_q)
         t_sim = time.perf_counter() - t0
         with S.MLPEnsemble(4, cuda_device) as ens:
             sur = S.Surrogate(ens, sim, tolerance=0.01)
-            sur.fit(train_q, train_s, steps=12000, batch=256, lr=2e-3, seed=0)
+            sur.fit(train_q, train_s, steps=36000, batch=256, lr=2e-3, seed=0)
             sur.query(test_q[:8])  # warm-up
             sig, fb, spread, t = sur.query(test_q)
+            # the network's answers alone, every query
+            each, _, _ = ens.predict(S.features(test_q))
+            nn_err = (np.abs(S.untarget(test_q, each).mean(axis=0) - truth) / np.abs(truth)).max(axis=1)
         err = (np.abs(sig - truth) / np.abs(truth)).max(axis=1)
         answered = ~fb
-        assert answered.mean() >= 0.5, answered.mean()
+        assert answered.mean() >= 0.9, answered.mean()
         # the network's own answers: within the tolerance where its members agree
         assert np.quantile(err[answered], 0.95) <= 0.01, np.quantile(err[answered], 0.95)
         assert err[answered].max() <= 0.03, err[answered].max()
+        assert np.quantile(nn_err, 0.95) <= 0.0125, np.quantile(nn_err, 0.95)
         # fallback answers are the simulator's
         assert err[fb].max(initial=0.0) <= 1e-9
-        # median latency of a query: the network pass alone when it answers
-        assert t_sim / t["network_s"] >= 20, (t_sim, t)
+        # latency of a query batch: the network pass alone when it answers
+        assert t_sim / t["network_s"] >= 100, (t_sim, t)
     finally:
         sim.close()

@@ -67,3 +67,16 @@ def test_features_and_targets():
         S.targets(q[:1], -sigma[:1])
     # the Drude scale is linear in tau
     assert S.sigma0(2e-12) == pytest.approx(2 * S.sigma0(1e-12))
+
+
+def test_training_draw_stays_in_the_config4_ranges():
+    q = S.training_queries(4000, seed=3)
+    assert q.shape == (4000, 5)
+    assert (q[:, 0] >= S.B_RANGE[0]).all() and (q[:, 0] <= S.B_RANGE[1]).all()
+    assert (q[:, 1] >= S.T_RANGE[0]).all() and (q[:, 1] <= S.T_RANGE[1]).all()
+    assert (q[:, 2] >= S.N_RANGE[0]).all() and (q[:, 2] <= S.N_RANGE[1]).all()
+    assert (q[:, 4] >= S.TAU_RANGE[0]).all() and (q[:, 4] <= S.TAU_RANGE[1]).all()
+    hard = q[2000:]
+    in_hard = ((hard[:, 0] <= S.HARD_B[1]) | (hard[:, 4] >= S.HARD_TAU[0]) | (hard[:, 1] <= S.HARD_T[1]))
+    assert in_hard.all()
+    assert np.array_equal(S.training_queries(100, seed=3, hard_fraction=0.0), S.sample_queries(100, seed=3))
