@@ -14,6 +14,8 @@ PKG = Path(__file__).resolve().parent
 
 ES_OK = 0
 ES_ERR_BAD_ARG = 1
+ES_ERR_OOM = 2
+ES_ERR_LAUNCH = 3
 STATUS_NAMES = {
     0: "ES_OK", 1: "ES_ERR_BAD_ARG", 2: "ES_ERR_OOM", 3: "ES_ERR_LAUNCH", 4: "ES_ERR_WALK_CAP",
     5: "ES_ERR_DEVICE", 6: "ES_ERR_NO_GRID", 7: "ES_ERR_NO_SAMPLE", 8: "ES_ERR_TIMEOUT",
@@ -112,6 +114,8 @@ CUDA_API = {
     "es_launch_count": (_i64, [_vp]),
     "es_probe_fp64_fma": (_i32, [_i32, C.POINTER(_d)]),
     "es_probe_fp32_fma": (_i32, [_i32, C.POINTER(_d)]),
+    "es_fault_inject": (_i32, [C.c_char_p]),
+    "es_fault_counts": (_i32, [C.POINTER(_i64)]),
     "es_derive_temperatures_noalloc": (_i32, [_vp, _i32, _i32, C.POINTER(Settings), _i32, _d, _vp, _i32, _vp, _vp]),
     "es_batch_create": (_i32, [_i32, C.POINTER(_vp)]),
     "es_batch_destroy": (_i32, [_vp]),
@@ -194,6 +198,22 @@ def cuda_lib() -> C.CDLL:
 def host_lib() -> C.CDLL:
     cuda_lib()
     return _load("libes_host.so", HOST_API)
+
+
+def fault_inject(spec: str | None) -> None:
+    """Arms host-side fault injection (es_fault_inject): "alloc:N", "copy:N",
+    "launch:N" items, comma-separated, "+" after N for "and every later one";
+    None or "" disarms."""
+    st = cuda_lib().es_fault_inject(spec.encode() if spec else None)
+    if st != ES_OK:
+        raise EsError(st, cuda_lib().es_last_error(None).decode())
+
+
+def fault_counts() -> dict:
+    """Operations counted since the last fault_inject, and how many failed."""
+    out = (_i64 * 4)()
+    cuda_lib().es_fault_counts(out)
+    return {"alloc": out[0], "copy": out[1], "launch": out[2], "failed": out[3]}
 
 
 def check(status: int, ctx=None) -> None:

@@ -41,6 +41,7 @@
 // is FP64. ES_PRECISION_FP64: stage (a) is the plain FP64 TraceOrbit and the
 // Boltzmann kernel is the FP64 expression of the per-pass path (es_integrate.cu).
 #include "es_cuda.h"
+#include "es_nvtx.h"
 #include "es_host_math.h"
 #include "es_orbit_split.cuh"
 #include "es_sigma32.cuh"
@@ -393,7 +394,7 @@ template <int kPrec, int kMinBlocks>
 cudaError_t launch_batch_t(const BatchLaunch& B, int n_sm, cudaStream_t s)
 {
     batch_kernel<kPrec, kMinBlocks><<<n_sm * kMinBlocks, kBatchWarps * 32, 0, s>>>(B);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 // ES_BATCH_PERSISTENT: the one kernel over every pass.
@@ -410,7 +411,7 @@ cudaError_t launch_batch(const BatchLaunch& B, int precision, int blocks_per_sm,
 cudaError_t launch_retrace(const BatchLaunch& B, int n_sm, cudaStream_t s)
 {
     batch_retrace_kernel<<<n_sm * 2, 256, 0, s>>>(B);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 }  // namespace
@@ -479,10 +480,7 @@ struct es_batch {
     // slot per distinct tau) and the scratch the single-pass kernels share
     double* d_psigma = nullptr;
     double* h_psigma = nullptr;                // pinned
-    // three passes' lifetimes in rotation: pass p writes d_lt[p % 3] and, split,
-    // reads the lifetimes of the pass one or two before it over the same orbits
-    // (another field) as its walk-length prediction
-    double* d_lt[3] = {};
+    double* d_lt = nullptr;                    // one pass's lifetimes
     long long lt_cap = 0;
     double4* d_otab = nullptr;                 // one pass's orbit table (split)
     long long otab_cap = 0;
@@ -545,12 +543,10 @@ void free_tables(es_batch* b)
 
 void free_pass_scratch(es_batch* b)
 {
-    for (double*& p : b->d_lt) {
-        cudaFree(p);
-        p = nullptr;
-    }
+    cudaFree(b->d_lt);
     cudaFree(b->d_otab);
     cudaFree(b->d_partial);
+    b->d_lt = nullptr;
     b->d_otab = nullptr;
     b->d_partial = nullptr;
     b->lt_cap = b->otab_cap = 0;
@@ -580,14 +576,14 @@ es_status ensure_capacity(es_batch* b, int64_t n)
     while (cap < n) cap *= 2;
     b->inst_offset = (size_t)((1 + cap + 1) * sizeof(long long) + 255) & ~(size_t)255;
     b->table_bytes = b->inst_offset + sizeof(es::BatchInstanceD) * (size_t)cap;
-    ES_BCUDA(cudaMalloc(&b->d_table, b->table_bytes), "batch table");
-    ES_BCUDA(cudaMallocHost(&b->h_table, b->table_bytes), "batch table (host)");
-    ES_BCUDA(cudaMalloc(&b->d_acc, sizeof(unsigned long long) * 2 * es::kBatchMaxTau * cap), "batch accumulators");
-    ES_BCUDA(cudaMalloc(&b->d_metrics, sizeof(unsigned long long) * es::kMetCount * cap), "batch metrics");
-    ES_BCUDA(cudaMallocHost(&b->h_acc, sizeof(unsigned long long) * 2 * es::kBatchMaxTau * cap), "batch accumulators");
-    ES_BCUDA(cudaMallocHost(&b->h_metrics, sizeof(unsigned long long) * es::kMetCount * cap), "batch metrics");
-    ES_BCUDA(cudaMalloc(&b->d_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap), "per-pass sigma");
-    ES_BCUDA(cudaMallocHost(&b->h_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap), "per-pass sigma (host)");
+    ES_BCUDA(es::dev_malloc(&b->d_table, b->table_bytes), "batch table");
+    ES_BCUDA(es::host_malloc(&b->h_table, b->table_bytes), "batch table (host)");
+    ES_BCUDA(es::dev_malloc(&b->d_acc, sizeof(unsigned long long) * 2 * es::kBatchMaxTau * cap), "batch accumulators");
+    ES_BCUDA(es::dev_malloc(&b->d_metrics, sizeof(unsigned long long) * es::kMetCount * cap), "batch metrics");
+    ES_BCUDA(es::host_malloc(&b->h_acc, sizeof(unsigned long long) * 2 * es::kBatchMaxTau * cap), "batch accumulators");
+    ES_BCUDA(es::host_malloc(&b->h_metrics, sizeof(unsigned long long) * es::kMetCount * cap), "batch metrics");
+    ES_BCUDA(es::dev_malloc(&b->d_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap), "per-pass sigma");
+    ES_BCUDA(es::host_malloc(&b->h_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap), "per-pass sigma (host)");
     std::memset(b->h_table, 0, b->table_bytes);
     b->cap = cap;
     return ES_OK;
@@ -601,7 +597,7 @@ es_status ensure_retrace(es_batch* b, long long want)
     cudaFree(b->d_retrace);
     b->d_retrace = nullptr;
     b->retrace_cap = 0;
-    ES_BCUDA(cudaMalloc(&b->d_retrace, sizeof(unsigned long long) * (size_t)want), "re-trace list");
+    ES_BCUDA(es::dev_malloc(&b->d_retrace, sizeof(unsigned long long) * (size_t)want), "re-trace list");
     b->retrace_cap = want;
     return ES_OK;
 }
@@ -619,9 +615,9 @@ es_status ensure_pass_scratch(es_batch* b)
     if (max_orbits <= b->lt_cap && max_phase <= b->otab_cap && b->d_partial) return ES_OK;
     drop_graph(b);
     free_pass_scratch(b);
-    for (double*& p : b->d_lt) ES_BCUDA(cudaMalloc(&p, sizeof(double) * (size_t)max_orbits), "pass lifetimes");
-    ES_BCUDA(cudaMalloc(&b->d_otab, sizeof(double4) * (size_t)max_phase), "pass orbit table");
-    ES_BCUDA(cudaMalloc(&b->d_partial, sizeof(double) * 2 * es::kMaxTChunk * es::kIntegrateBlocks),
+    ES_BCUDA(es::dev_malloc(&b->d_lt, sizeof(double) * (size_t)max_orbits), "pass lifetimes");
+    ES_BCUDA(es::dev_malloc(&b->d_otab, sizeof(double4) * (size_t)max_phase), "pass orbit table");
+    ES_BCUDA(es::dev_malloc(&b->d_partial, sizeof(double) * 2 * es::kMaxTChunk * es::kIntegrateBlocks),
              "integration partials");
     b->lt_cap = max_orbits;
     b->otab_cap = max_phase;
@@ -641,25 +637,8 @@ cudaError_t record_pass_kernels(es_batch* b)
         const int k = b->order[pos];
         const es_batch_grid& g = b->grids[(size_t)b->inst[(size_t)k].grid];
         es::LifetimeLaunch L = d.L;
-        L.out = b->d_lt[pos % 3];
+        L.out = b->d_lt;
         L.out32 = nullptr;
-        L.pred = nullptr;
-        if (b->tuning.precision == ES_PRECISION_SPLIT) {
-            // the nearest of the two passes before this one over the same orbits
-            const es_batch_instance& x = b->inst[(size_t)k];
-            for (size_t q = pos; q-- > 0 && q + 2 >= pos;) {
-                const es_batch_instance& y = b->inst[(size_t)b->order[q]];
-                if (y.grid == x.grid && y.positions_per_row == x.positions_per_row &&
-                    y.particles_per_quadrant == x.particles_per_quadrant && y.coherent == x.coherent &&
-                    y.region_size == x.region_size && y.grid_cell_size == x.grid_cell_size &&
-                    y.settings.alpha == x.settings.alpha && y.settings.is_clockwise == x.settings.is_clockwise &&
-                    y.settings.particle_speed == x.settings.particle_speed) {
-                    L.pred = b->d_lt[q % 3];
-                    L.pred_scale = x.settings.particle_speed / g.is.cell_size;
-                    break;
-                }
-            }
-        }
         L.metrics = d.metrics;
         L.row0 = 0;
         L.variant = es::kLifetimePerThreadDefer;
@@ -675,7 +654,7 @@ cudaError_t record_pass_kernels(es_batch* b)
             e = es::launch_lifetimes_fp64(L, b->stream);
         if (e != cudaSuccess) break;
         es::IntegrateLaunch I{};
-        I.lifetimes = b->d_lt[pos % 3];
+        I.lifetimes = b->d_lt;
         I.phase = d.phase_sigma;
         for (int u = 0; u < d.n_tau; u++) {
             I.tau[u] = d.tau[u];
@@ -701,6 +680,7 @@ cudaError_t record_pass_kernels(es_batch* b)
 // pass kernels, the FP64 re-trace, readbacks.
 es_status capture(es_batch* b)
 {
+    es::Range nvtx_range("batch_record");
     drop_graph(b);
     es_status st = ES_OK;
     if (b->tuning.mode == ES_BATCH_PASS_KERNELS && (st = ensure_pass_scratch(b)) != ES_OK) return st;
@@ -719,7 +699,7 @@ es_status capture(es_batch* b)
     const size_t met_bytes = sizeof(unsigned long long) * es::kMetCount * cap;
 
     ES_BCUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
-    cudaError_t e = cudaMemcpyAsync(b->d_table, b->h_table, b->table_bytes, cudaMemcpyHostToDevice, b->stream);
+    cudaError_t e = es::copy_async(b->d_table, b->h_table, b->table_bytes, cudaMemcpyHostToDevice, b->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_acc, 0, acc_bytes, b->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_metrics, 0, met_bytes, b->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), b->stream);
@@ -732,13 +712,13 @@ es_status capture(es_batch* b)
     if (e == cudaSuccess && b->tuning.precision == ES_PRECISION_SPLIT && b->tuning.mode != ES_BATCH_PASS_KERNELS)
         e = es::launch_retrace(L, b->n_sm, b->stream);
     if (e == cudaSuccess && b->tuning.mode == ES_BATCH_PASS_KERNELS)
-        e = cudaMemcpyAsync(b->h_psigma, b->d_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap,
+        e = es::copy_async(b->h_psigma, b->d_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap,
                             cudaMemcpyDeviceToHost, b->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_acc, b->d_acc, acc_bytes, cudaMemcpyDeviceToHost, b->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_metrics, b->d_metrics, met_bytes, cudaMemcpyDeviceToHost, b->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_error, b->d_error, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = es::copy_async(b->h_acc, b->d_acc, acc_bytes, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = es::copy_async(b->h_metrics, b->d_metrics, met_bytes, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = es::copy_async(b->h_error, b->d_error, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(b->h_retrace_count, b->d_retrace_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+        e = es::copy_async(b->h_retrace_count, b->d_retrace_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             b->stream);
     cudaGraph_t g = nullptr;
     const cudaError_t e_end = cudaStreamEndCapture(b->stream, &g);
@@ -773,6 +753,7 @@ double fixed_point_scale(int dim, int ppq, double max_wtau)
 
 es_status add_grid_arrays(es_batch* b, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
                           const es_impurity_settings* is, cudaMemcpyKind kind, int32_t* out_grid);
+es_status lay_instances(es_batch* b, const es_batch_instance* inst, int32_t n);
 
 }  // namespace
 
@@ -780,6 +761,7 @@ extern "C" {
 
 es_status es_batch_create(int32_t device_ordinal, es_batch** out)
 {
+    es::Range nvtx_range("batch_create");
     if (!out) return ES_ERR_BAD_ARG;
     *out = nullptr;
     int n_dev = 0;
@@ -802,11 +784,11 @@ es_status es_batch_create(int32_t device_ordinal, es_batch** out)
     b->n_sm = prop.multiProcessorCount;
     cudaError_t e = cudaSetDevice(device_ordinal);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_error, sizeof(int));
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_error, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_retrace_count, sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_retrace_count, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = es::dev_malloc(&b->d_counter, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = es::dev_malloc(&b->d_error, sizeof(int));
+    if (e == cudaSuccess) e = es::host_malloc(&b->h_error, sizeof(int));
+    if (e == cudaSuccess) e = es::dev_malloc(&b->d_retrace_count, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = es::host_malloc(&b->h_retrace_count, sizeof(unsigned long long));
     if (e == cudaSuccess) {
         *b->h_error = 0;
         *b->h_retrace_count = 0;
@@ -866,12 +848,20 @@ es_status es_batch_set_tuning(es_batch* b, const es_batch_tuning* t)
         return x.mode == ES_BATCH_PERSISTENT ? 32LL * x.chunk_iters : 32LL * es::kBatchWarps;
     };
     const bool items_change = item_orbits(*t) != item_orbits(b->tuning);
+    const es_batch_tuning old = b->tuning;
     b->tuning = *t;
     b->graph_dirty = true;
-    if (items_change && b->has_instances) {
-        // work-item boundaries depend on the mode and chunk_iters: re-lay the table
+    if (items_change && !b->inst.empty()) {
+        // work-item boundaries depend on the mode and chunk_iters: re-lay the table.
+        // On failure the old tuning stays and the instance list is kept, so the
+        // same call can be repeated; until then the batch runs nothing.
         std::vector<es_batch_instance> copy = b->inst;
-        return es_batch_set_instances(b, copy.data(), (int32_t)copy.size());
+        const es_status st = lay_instances(b, copy.data(), (int32_t)copy.size());
+        if (st != ES_OK) {
+            b->tuning = old;
+            b->inst = copy;
+        }
+        return st;
     }
     return ES_OK;
 }
@@ -879,6 +869,7 @@ es_status es_batch_set_tuning(es_batch* b, const es_batch_tuning* t)
 es_status es_batch_add_grid(es_batch* b, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
                             const es_impurity_settings* is, int32_t* out_grid)
 {
+    es::Range nvtx_range("batch_add_grid");
     es_status st = bind_batch(b);
     if (st != ES_OK) return st;
     if (!is || !cell_end || !out_grid || n_indexed < 0 || (n_indexed > 0 && !imp_xy))
@@ -900,6 +891,7 @@ es_status es_batch_add_grid(es_batch* b, const double* imp_xy, int64_t n_indexed
 
 es_status es_batch_add_dgrid(es_batch* b, const es_dgrid* grid, int32_t* out_grid)
 {
+    es::Range nvtx_range("batch_add_grid");
     es_status st = bind_batch(b);
     if (st != ES_OK) return st;
     if (!grid || !out_grid) return bfail(b, ES_ERR_BAD_ARG, "es_batch_add_dgrid: null argument");
@@ -930,11 +922,11 @@ es_status add_grid_arrays(es_batch* b, const double* imp_xy, int64_t n_indexed, 
     g.n_indexed = n_indexed;
     g.is = *is;
     const size_t n_alloc = (size_t)(n_indexed > 0 ? n_indexed : 1);
-    cudaError_t e = cudaMalloc(&g.d_imps, sizeof(double2) * n_alloc);
-    if (e == cudaSuccess) e = cudaMalloc(&g.d_imps32, sizeof(float2) * n_alloc);
-    if (e == cudaSuccess) e = cudaMalloc(&g.d_cell_end, sizeof(int) * n_cells);
-    if (e == cudaSuccess && n_indexed > 0) e = cudaMemcpyAsync(g.d_imps, imp_xy, sizeof(double2) * n_indexed, kind, b->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(g.d_cell_end, cell_end, sizeof(int) * n_cells, kind, b->stream);
+    cudaError_t e = es::dev_malloc(&g.d_imps, sizeof(double2) * n_alloc);
+    if (e == cudaSuccess) e = es::dev_malloc(&g.d_imps32, sizeof(float2) * n_alloc);
+    if (e == cudaSuccess) e = es::dev_malloc(&g.d_cell_end, sizeof(int) * n_cells);
+    if (e == cudaSuccess && n_indexed > 0) e = es::copy_async(g.d_imps, imp_xy, sizeof(double2) * n_indexed, kind, b->stream);
+    if (e == cudaSuccess) e = es::copy_async(g.d_cell_end, cell_end, sizeof(int) * n_cells, kind, b->stream);
     if (e == cudaSuccess)
         e = es::launch_local_impurities(g.d_imps, g.d_cell_end, g.d_imps32, is->spawn_region_start, is->cell_size,
                                         is->cells_per_row, b->stream);
@@ -967,6 +959,19 @@ es_status es_batch_clear(es_batch* b)
 }
 
 es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int32_t n)
+{
+    es::Range nvtx_range("batch_set_instances");
+    const es_status st = lay_instances(b, inst, n);
+    // a failure after the table was touched leaves no instances to run
+    if (st != ES_OK && b && !b->has_instances) b->inst.clear();
+    return st;
+}
+
+}  // extern "C"
+
+namespace {
+
+es_status lay_instances(es_batch* b, const es_batch_instance* inst, int32_t n)
 {
     namespace H = es::host;
     es_status st = bind_batch(b);
@@ -1038,12 +1043,12 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
                             po.data(), psg.data());
             es_batch_phase p;
             p.phi_integrand_factor = sec.phi_integrand_factor;
-            cudaError_t e = cudaMalloc(&p.d_orbit, sizeof(es::PhaseOrbit) * po.size());
-            if (e == cudaSuccess) e = cudaMalloc(&p.d_sigma, sizeof(es::PhaseSigma) * psg.size());
+            cudaError_t e = es::dev_malloc(&p.d_orbit, sizeof(es::PhaseOrbit) * po.size());
+            if (e == cudaSuccess) e = es::dev_malloc(&p.d_sigma, sizeof(es::PhaseSigma) * psg.size());
             if (e == cudaSuccess)
-                e = cudaMemcpy(p.d_orbit, po.data(), sizeof(es::PhaseOrbit) * po.size(), cudaMemcpyHostToDevice);
+                e = es::copy_sync(p.d_orbit, po.data(), sizeof(es::PhaseOrbit) * po.size(), cudaMemcpyHostToDevice);
             if (e == cudaSuccess)
-                e = cudaMemcpy(p.d_sigma, psg.data(), sizeof(es::PhaseSigma) * psg.size(), cudaMemcpyHostToDevice);
+                e = es::copy_sync(p.d_sigma, psg.data(), sizeof(es::PhaseSigma) * psg.size(), cudaMemcpyHostToDevice);
             if (e != cudaSuccess) {
                 cudaFree(p.d_orbit);
                 cudaFree(p.d_sigma);
@@ -1054,6 +1059,10 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
         ph[(size_t)k] = &it->second;
     }
 
+    // From here the instance table is rewritten: until it is complete the batch
+    // has no instances, so a failure below leaves nothing that es_batch_enqueue
+    // would run.
+    b->has_instances = false;
     if ((st = ensure_capacity(b, n)) != ES_OK) return st;
 
     // kernel order: largest passes first, so the tail of the run is made of small work items
@@ -1143,18 +1152,23 @@ es_status es_batch_set_instances(es_batch* b, const es_batch_instance* inst, int
     b->t_slot = t_slot;
     b->total_orbits = total;
     b->total_items = items;
-    b->has_instances = true;
-    // pass records are kernel parameters in this mode: record the graph again
-    if (b->tuning.mode == ES_BATCH_PASS_KERNELS) b->graph_dirty = true;
     // Re-traced orbits are a small fraction (observed ~0.05%); the list starts
     // at 1/1024 of the run and grows on overflow (es_batch_collect re-runs).
     if (b->tuning.precision == ES_PRECISION_SPLIT)
         if ((st = ensure_retrace(b, total / 1024 + 262144)) != ES_OK) return st;
+    b->has_instances = true;
+    // pass records are kernel parameters in this mode: record the graph again
+    if (b->tuning.mode == ES_BATCH_PASS_KERNELS) b->graph_dirty = true;
     return ES_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
 es_status es_batch_enqueue(es_batch* b)
 {
+    es::Range nvtx_range("batch_enqueue");
     es_status st = bind_batch(b);
     if (st != ES_OK) return st;
     if (!b->has_instances) return bfail(b, ES_ERR_BAD_ARG, "es_batch_set_instances has not been called");
@@ -1169,6 +1183,7 @@ es_status es_batch_enqueue(es_batch* b)
 
 es_status es_batch_collect(es_batch* b, double* out_sigma, es_metrics* out_metrics)
 {
+    es::Range nvtx_range("batch_collect");
     es_status st = bind_batch(b);
     if (st != ES_OK) return st;
     if (!b->has_instances) return bfail(b, ES_ERR_BAD_ARG, "es_batch_set_instances has not been called");

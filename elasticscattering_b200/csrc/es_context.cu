@@ -8,6 +8,7 @@
 // exactly like the reference's CPU code.
 #include "es_cuda.h"
 #include "es_host_math.h"
+#include "es_nvtx.h"
 #include "es_internal.h"
 
 #include <cfloat>
@@ -16,7 +17,6 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
-#include <utility>
 #include <vector>
 
 namespace {
@@ -55,11 +55,6 @@ struct es_ctx {
     int n_phase = 0;
     int n_pos = 0;
     double* d_lifetimes = nullptr;
-    // split precision: the previous pass's lifetimes (same grid, sector and rows,
-    // another field), the walk-length prediction of the next pass; the two
-    // buffers swap roles every pass
-    double* d_prev = nullptr;
-    bool prev_valid = false;
     es::PhaseOrbit* d_phase_orbit = nullptr;
     double4* d_orbit_table = nullptr;  // split precision: the pass's per-phase orbit table
     es::PhaseSigma* d_phase_sigma = nullptr;
@@ -170,8 +165,6 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.retrace_cap = ctx->retrace_cap;
     L.orbit_table = ctx->d_orbit_table;
     es::host::split_constants(L);
-    L.pred = nullptr;
-    L.pred_scale = speed / ctx->is.cell_size;
     return L;
 }
 
@@ -185,17 +178,11 @@ es_status enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
     if (ctx->desc.precision == ES_PRECISION_SPLIT) {
         const bool defer = es::host::long_walks(ctx->n_imps, ctx->is.cells_per_row, ctx->is.cell_size,
                                                 ctx->is.impurity_radius);
-        es::LifetimeLaunch Ls = L;
-        if (ctx->prev_valid && ctx->d_prev) {
-            // this pass writes the other buffer and reads the last pass's lifetimes
-            std::swap(ctx->d_lifetimes, ctx->d_prev);
-            Ls.out = ctx->d_lifetimes;
-            Ls.pred = ctx->d_prev;
-        }
-        ES_CUDA(es::launch_lifetimes_split(Ls, defer, ctx->stream), "split lifetime kernel launch");
+        ctx->lifetimes_valid = false;  // set again once every launch of the pass is made
+        ES_CUDA(es::launch_lifetimes_split(L, defer, ctx->stream), "split lifetime kernel launch");
         ctx->launches += 3;  // orbit table, lifetime walk, FP64 re-trace
-        ctx->prev_valid = ctx->d_prev != nullptr;
     } else {
+        ctx->lifetimes_valid = false;
         ES_CUDA(es::launch_lifetimes_fp64(L, ctx->stream), "lifetime kernel launch");
         ctx->launches++;
     }
@@ -264,7 +251,7 @@ es_status enqueue_integrate(es_ctx* ctx, const double* temperatures, int32_t n_t
 es_status read_device_error(es_ctx* ctx)
 {
     int h_err = 0;
-    ES_CUDA(cudaMemcpyAsync(&h_err, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "error readback");
+    ES_CUDA(es::copy_async(&h_err, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "error readback");
     ES_CUDA(cudaStreamSynchronize(ctx->stream), "stream synchronize");
     if (h_err) {
         ES_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream), "error reset");
@@ -280,7 +267,7 @@ es_status read_device_error(es_ctx* ctx)
 es_status read_metrics_into(es_ctx* ctx, es_metrics* out, bool reset)
 {
     unsigned long long h[es::kMetCount];
-    ES_CUDA(cudaMemcpyAsync(h, ctx->d_metrics, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "metrics readback");
+    ES_CUDA(es::copy_async(h, ctx->d_metrics, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "metrics readback");
     if (reset) ES_CUDA(cudaMemsetAsync(ctx->d_metrics, 0, sizeof(h), ctx->stream), "metrics reset");
     ES_CUDA(cudaStreamSynchronize(ctx->stream), "stream synchronize");
     if (out) {
@@ -305,7 +292,7 @@ es_status ensure_pos(es_ctx* ctx, int32_t n_t)
     if (ctx->d_pos) cudaFree(ctx->d_pos);
     ctx->d_pos = nullptr;
     ctx->pos_cap = 0;
-    ES_CUDA(cudaMalloc(&ctx->d_pos, sizeof(double) * 3 * need), "image buffers");
+    ES_CUDA(es::dev_malloc(&ctx->d_pos, sizeof(double) * 3 * need), "image buffers");
     ctx->pos_cap = need;
     return ES_OK;
 }
@@ -318,7 +305,6 @@ void release(es_ctx* ctx)
     cudaFree(ctx->d_imps);
     cudaFree(ctx->d_cell_end);
     cudaFree(ctx->d_lifetimes);
-    cudaFree(ctx->d_prev);
     cudaFree(ctx->d_phase_orbit);
     cudaFree(ctx->d_orbit_table);
     cudaFree(ctx->d_phase_sigma);
@@ -344,6 +330,7 @@ extern "C" {
 
 es_status es_create(const es_sim_desc* desc, es_ctx** out)
 {
+    es::Range nvtx_range("create");
     if (!desc || !out) return fail(nullptr, ES_ERR_BAD_ARG, "null argument");
     *out = nullptr;
     if (desc->positions_per_row < 3 || desc->positions_per_row % 2 == 0)
@@ -384,25 +371,23 @@ es_status es_create(const es_sim_desc* desc, es_ctx** out)
 
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_lifetimes, sizeof(double) * ctx->n_orbits);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_phase_orbit, sizeof(es::PhaseOrbit) * n_phase);
+    if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_lifetimes, sizeof(double) * ctx->n_orbits);
+    if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_phase_orbit, sizeof(es::PhaseOrbit) * n_phase);
     if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT)
-        e = cudaMalloc(&ctx->d_orbit_table, sizeof(double4) * n_phase);
-    if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT)
-        e = cudaMalloc(&ctx->d_prev, sizeof(double) * ctx->n_orbits);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_phase_sigma, sizeof(es::PhaseSigma) * n_phase);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_metrics, sizeof(unsigned long long) * es::kMetCount);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(int));
+        e = es::dev_malloc(&ctx->d_orbit_table, sizeof(double4) * n_phase);
+    if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_phase_sigma, sizeof(es::PhaseSigma) * n_phase);
+    if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_metrics, sizeof(unsigned long long) * es::kMetCount);
+    if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_error, sizeof(int));
     if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT) {
         // Re-traced orbits are a small fraction (guard-band decisions); a quarter
         // of the pass is a generous bound, and overflow is reported, not ignored.
         ctx->retrace_cap = ctx->n_orbits / 4 + 1024;
-        e = cudaMalloc(&ctx->d_retrace, sizeof(long long) * ctx->retrace_cap);
-        if (e == cudaSuccess) e = cudaMalloc(&ctx->d_retrace_count, sizeof(unsigned long long));
+        e = es::dev_malloc(&ctx->d_retrace, sizeof(long long) * ctx->retrace_cap);
+        if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_retrace_count, sizeof(unsigned long long));
     }
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_partial, sizeof(double) * 2 * es::kMaxTChunk * es::kIntegrateBlocks);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_sigma, sizeof(double) * 2 * es::kMaxTChunk);
-    if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_sigma, sizeof(double) * 2 * es::kMaxTChunk);
+    if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_partial, sizeof(double) * 2 * es::kMaxTChunk * es::kIntegrateBlocks);
+    if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_sigma, sizeof(double) * 2 * es::kMaxTChunk);
+    if (e == cudaSuccess) e = es::host_malloc(&ctx->h_sigma, sizeof(double) * 2 * es::kMaxTChunk);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_metrics, 0, sizeof(unsigned long long) * es::kMetCount, ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -435,30 +420,35 @@ es_status upload_arrays(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, co
                         const es_impurity_settings* is, uint64_t generation, cudaMemcpyKind kind)
 {
     const int64_t n_cells = (int64_t)is->cells_per_row * is->cells_per_row;
+    // Until this upload completes the context holds no usable grid: a failure
+    // below leaves it asking for es_upload_grid again, so no launch can pair
+    // the old grid's settings with partly replaced arrays.
+    ctx->has_grid = false;
+    ctx->lifetimes_valid = false;
     if (n_indexed > ctx->imps_cap) {
         cudaFree(ctx->d_imps);
         ctx->d_imps = nullptr;
         ctx->imps_cap = 0;
-        ES_CUDA(cudaMalloc(&ctx->d_imps, sizeof(double2) * (n_indexed > 0 ? n_indexed : 1)), "impurity buffer");
+        ES_CUDA(es::dev_malloc(&ctx->d_imps, sizeof(double2) * (n_indexed > 0 ? n_indexed : 1)), "impurity buffer");
         ctx->imps_cap = n_indexed;
     }
     if (n_cells > ctx->cells_cap) {
         cudaFree(ctx->d_cell_end);
         ctx->d_cell_end = nullptr;
         ctx->cells_cap = 0;
-        ES_CUDA(cudaMalloc(&ctx->d_cell_end, sizeof(int) * n_cells), "cell index buffer");
+        ES_CUDA(es::dev_malloc(&ctx->d_cell_end, sizeof(int) * n_cells), "cell index buffer");
         ctx->cells_cap = n_cells;
     }
     if (n_indexed > 0)
-        ES_CUDA(cudaMemcpyAsync(ctx->d_imps, imp_xy, sizeof(double2) * n_indexed, kind, ctx->stream),
+        ES_CUDA(es::copy_async(ctx->d_imps, imp_xy, sizeof(double2) * n_indexed, kind, ctx->stream),
                 "impurity upload");
-    ES_CUDA(cudaMemcpyAsync(ctx->d_cell_end, cell_end, sizeof(int) * n_cells, kind, ctx->stream), "cell index upload");
+    ES_CUDA(es::copy_async(ctx->d_cell_end, cell_end, sizeof(int) * n_cells, kind, ctx->stream), "cell index upload");
     if (ctx->desc.precision == ES_PRECISION_SPLIT) {
         if (n_indexed > ctx->imps32_cap) {
             cudaFree(ctx->d_imps32);
             ctx->d_imps32 = nullptr;
             ctx->imps32_cap = 0;
-            ES_CUDA(cudaMalloc(&ctx->d_imps32, sizeof(float2) * (n_indexed > 0 ? n_indexed : 1)), "FP32 impurity buffer");
+            ES_CUDA(es::dev_malloc(&ctx->d_imps32, sizeof(float2) * (n_indexed > 0 ? n_indexed : 1)), "FP32 impurity buffer");
             ctx->imps32_cap = n_indexed;
         }
         ES_CUDA(es::launch_local_impurities(ctx->d_imps, ctx->d_cell_end, ctx->d_imps32, is->spawn_region_start,
@@ -472,7 +462,6 @@ es_status upload_arrays(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, co
     ctx->generation = generation;
     ctx->has_grid = true;
     ctx->lifetimes_valid = false;
-    ctx->prev_valid = false;
     return ES_OK;
 }
 
@@ -505,13 +494,13 @@ es_status es_set_rows(es_ctx* ctx, int32_t j0, int32_t j1)
     ctx->row0 = j0;
     ctx->row1 = j1;
     ctx->lifetimes_valid = false;
-    ctx->prev_valid = false;
     return ES_OK;
 }
 
 es_status es_upload_grid(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
                          const es_impurity_settings* is, uint64_t generation)
 {
+    es::Range nvtx_range("upload_grid");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if (!is || !cell_end || n_indexed < 0 || (n_indexed > 0 && !imp_xy))
@@ -536,6 +525,7 @@ es_status es_upload_grid(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, c
 
 es_status es_upload_dgrid(es_ctx* ctx, const es_dgrid* g)
 {
+    es::Range nvtx_range("upload_grid");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if (!g) return fail(ctx, ES_ERR_BAD_ARG, "es_upload_dgrid: null grid");
@@ -557,6 +547,7 @@ es_status es_upload_dgrid(es_ctx* ctx, const es_dgrid* g)
 
 es_status es_init_sample(es_ctx* ctx, const es_settings* s, int32_t coherent)
 {
+    es::Range nvtx_range("init_sample");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if (!s) return fail(ctx, ES_ERR_BAD_ARG, "es_init_sample: null settings");
@@ -582,6 +573,8 @@ es_status es_init_sample(es_ctx* ctx, const es_settings* s, int32_t coherent)
             }
     }
 
+    ctx->has_sample = false;  // until the phase tables below are on the device
+    ctx->lifetimes_valid = false;
     ctx->settings = *s;
     ctx->coherent = coherent ? 1 : 0;
 
@@ -596,28 +589,28 @@ es_status es_init_sample(es_ctx* ctx, const es_settings* s, int32_t coherent)
     std::vector<es::PhaseOrbit> po((size_t)ctx->n_phase);
     std::vector<es::PhaseSigma> psg((size_t)ctx->n_phase);
     es::host::phase_tables(sec, ppq, s->particle_speed, s->alpha, s->is_clockwise != 0, po.data(), psg.data());
-    ES_CUDA(cudaMemcpyAsync(ctx->d_phase_orbit, po.data(), sizeof(es::PhaseOrbit) * po.size(), cudaMemcpyHostToDevice,
+    ES_CUDA(es::copy_async(ctx->d_phase_orbit, po.data(), sizeof(es::PhaseOrbit) * po.size(), cudaMemcpyHostToDevice,
                             ctx->stream),
             "phase table upload");
-    ES_CUDA(cudaMemcpyAsync(ctx->d_phase_sigma, psg.data(), sizeof(es::PhaseSigma) * psg.size(),
+    ES_CUDA(es::copy_async(ctx->d_phase_sigma, psg.data(), sizeof(es::PhaseSigma) * psg.size(),
                             cudaMemcpyHostToDevice, ctx->stream),
             "phase table upload");
     ES_CUDA(cudaStreamSynchronize(ctx->stream), "phase table upload");
     ctx->has_sample = true;
     ctx->lifetimes_valid = false;
-    ctx->prev_valid = false;
     return ES_OK;
 }
 
 es_status es_compute_lifetimes(es_ctx* ctx, double magnetic_field, double* out_lifetimes, es_metrics* out_metrics)
 {
+    es::Range nvtx_range("lifetimes");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if ((st = check_ready(ctx)) != ES_OK) return st;
     ES_CUDA(cudaMemsetAsync(ctx->d_metrics, 0, sizeof(unsigned long long) * es::kMetCount, ctx->stream), "metrics reset");
     if ((st = enqueue_lifetimes(ctx, magnetic_field)) != ES_OK) return st;
     if (out_lifetimes)
-        ES_CUDA(cudaMemcpyAsync(out_lifetimes, ctx->d_lifetimes, sizeof(double) * ctx->n_orbits, cudaMemcpyDeviceToHost,
+        ES_CUDA(es::copy_async(out_lifetimes, ctx->d_lifetimes, sizeof(double) * ctx->n_orbits, cudaMemcpyDeviceToHost,
                                 ctx->stream),
                 "lifetime readback");
     if ((st = read_metrics_into(ctx, out_metrics, true)) != ES_OK) return st;
@@ -633,7 +626,7 @@ es_status es_read_lifetimes(es_ctx* ctx, int64_t first, int64_t count, double* o
         return fail(ctx, ES_ERR_BAD_ARG, "es_read_lifetimes: range [%lld, +%lld) outside the %lld orbits of the pass",
                     (long long)first, (long long)count, (long long)ctx->n_orbits);
     if (count == 0) return ES_OK;
-    ES_CUDA(cudaMemcpyAsync(out, ctx->d_lifetimes + first, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream),
+    ES_CUDA(es::copy_async(out, ctx->d_lifetimes + first, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream),
             "lifetime readback");
     ES_CUDA(cudaStreamSynchronize(ctx->stream), "lifetime readback");
     return ES_OK;
@@ -641,6 +634,7 @@ es_status es_read_lifetimes(es_ctx* ctx, int64_t first, int64_t count, double* o
 
 es_status es_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_t n_t, double* out_sigma)
 {
+    es::Range nvtx_range("temperatures");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if ((st = check_ready(ctx)) != ES_OK) return st;
@@ -650,7 +644,7 @@ es_status es_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_
     for (int32_t t0 = 0; t0 < n_t; t0 += es::kMaxTChunk) {
         const int nc = (n_t - t0) < es::kMaxTChunk ? (n_t - t0) : es::kMaxTChunk;
         if ((st = enqueue_integrate(ctx, temperatures + t0, nc, ctx->d_sigma, nullptr)) != ES_OK) return st;
-        ES_CUDA(cudaMemcpyAsync(ctx->h_sigma, ctx->d_sigma, sizeof(double) * 2 * nc, cudaMemcpyDeviceToHost, ctx->stream),
+        ES_CUDA(es::copy_async(ctx->h_sigma, ctx->d_sigma, sizeof(double) * 2 * nc, cudaMemcpyDeviceToHost, ctx->stream),
                 "sigma readback");
         ES_CUDA(cudaStreamSynchronize(ctx->stream), "sigma readback");
         std::memcpy(out_sigma + 2 * t0, ctx->h_sigma, sizeof(double) * 2 * nc);
@@ -661,6 +655,7 @@ es_status es_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_
 es_status es_compute_sigmas(es_ctx* ctx, double magnetic_field, const double* temperatures, int32_t n_t,
                             double* out_sigma, es_metrics* out_metrics)
 {
+    es::Range nvtx_range("compute_sigmas");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if ((st = check_ready(ctx)) != ES_OK) return st;
@@ -675,6 +670,7 @@ es_status es_compute_sigmas_images(es_ctx* ctx, double magnetic_field, const dou
                                    double* out_sigma, double* lifetime_pos, double* sigma_xx_pos,
                                    double* sigma_xy_pos, es_metrics* out_metrics)
 {
+    es::Range nvtx_range("compute_sigmas_images");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if ((st = check_ready(ctx)) != ES_OK) return st;
@@ -690,16 +686,16 @@ es_status es_compute_sigmas_images(es_ctx* ctx, double magnetic_field, const dou
         const int nc = (n_t - t0) < es::kMaxTChunk ? (n_t - t0) : es::kMaxTChunk;
         if ((st = enqueue_integrate(ctx, temperatures + t0, nc, ctx->d_sigma, ctx->d_pos)) != ES_OK) return st;
         const size_t bytes = sizeof(double) * (size_t)nc * ctx->n_pos;
-        ES_CUDA(cudaMemcpyAsync(lifetime_pos + (int64_t)t0 * ctx->n_pos, ctx->d_pos, bytes, cudaMemcpyDeviceToHost,
+        ES_CUDA(es::copy_async(lifetime_pos + (int64_t)t0 * ctx->n_pos, ctx->d_pos, bytes, cudaMemcpyDeviceToHost,
                                 ctx->stream),
                 "image readback");
-        ES_CUDA(cudaMemcpyAsync(sigma_xx_pos + (int64_t)t0 * ctx->n_pos, ctx->d_pos + ctx->pos_cap, bytes,
+        ES_CUDA(es::copy_async(sigma_xx_pos + (int64_t)t0 * ctx->n_pos, ctx->d_pos + ctx->pos_cap, bytes,
                                 cudaMemcpyDeviceToHost, ctx->stream),
                 "image readback");
-        ES_CUDA(cudaMemcpyAsync(sigma_xy_pos + (int64_t)t0 * ctx->n_pos, ctx->d_pos + 2 * ctx->pos_cap, bytes,
+        ES_CUDA(es::copy_async(sigma_xy_pos + (int64_t)t0 * ctx->n_pos, ctx->d_pos + 2 * ctx->pos_cap, bytes,
                                 cudaMemcpyDeviceToHost, ctx->stream),
                 "image readback");
-        ES_CUDA(cudaMemcpyAsync(ctx->h_sigma, ctx->d_sigma, sizeof(double) * 2 * nc, cudaMemcpyDeviceToHost, ctx->stream),
+        ES_CUDA(es::copy_async(ctx->h_sigma, ctx->d_sigma, sizeof(double) * 2 * nc, cudaMemcpyDeviceToHost, ctx->stream),
                 "sigma readback");
         ES_CUDA(cudaStreamSynchronize(ctx->stream), "image readback");
         std::memcpy(out_sigma + 2 * t0, ctx->h_sigma, sizeof(double) * 2 * nc);
@@ -710,6 +706,7 @@ es_status es_compute_sigmas_images(es_ctx* ctx, double magnetic_field, const dou
 es_status es_enqueue_sigmas(es_ctx* ctx, double magnetic_field, const double* temperatures, int32_t n_t,
                             double* d_out_sigma)
 {
+    es::Range nvtx_range("enqueue_sigmas");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if ((st = check_ready(ctx)) != ES_OK) return st;
@@ -721,6 +718,7 @@ es_status es_enqueue_sigmas(es_ctx* ctx, double magnetic_field, const double* te
 
 es_status es_enqueue_derive_temperatures(es_ctx* ctx, const double* temperatures, int32_t n_t, double* d_out_sigma)
 {
+    es::Range nvtx_range("enqueue_temperatures");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if ((st = check_ready(ctx)) != ES_OK) return st;
@@ -731,6 +729,7 @@ es_status es_enqueue_derive_temperatures(es_ctx* ctx, const double* temperatures
 
 es_status es_enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
 {
+    es::Range nvtx_range("enqueue_lifetimes");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if ((st = check_ready(ctx)) != ES_OK) return st;
@@ -739,6 +738,7 @@ es_status es_enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
 
 es_status es_average_lifetime(es_ctx* ctx, double* out_average)
 {
+    es::Range nvtx_range("average_lifetime");
     es_status st = bind(ctx);
     if (st != ES_OK) return st;
     if (!out_average) return fail(ctx, ES_ERR_BAD_ARG, "es_average_lifetime: null output");
@@ -748,7 +748,7 @@ es_status es_average_lifetime(es_ctx* ctx, double* out_average)
     ES_CUDA(es::launch_lifetime_sum(ctx->d_lifetimes, ctx->n_orbits, ctx->d_partial, ctx->d_sigma, ctx->stream),
             "lifetime sum");
     ctx->launches += 2;
-    ES_CUDA(cudaMemcpyAsync(ctx->h_sigma, ctx->d_sigma, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+    ES_CUDA(es::copy_async(ctx->h_sigma, ctx->d_sigma, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
             "lifetime sum readback");
     ES_CUDA(cudaStreamSynchronize(ctx->stream), "lifetime sum");
     *out_average = ctx->h_sigma[0] / (double)ctx->n_orbits;  // Simulation::AverageLifetime
@@ -791,10 +791,10 @@ es_status es_debug_trace(es_ctx* ctx, double px, double py, int32_t q, int32_t p
     const double remaining = es::host::smod(ph.phi + alpha, kHALF_PI);
     ph.bound_dphi = is_clockwise ? remaining : (2.0 * alpha - remaining);
     double* d = nullptr;
-    ES_CUDA(cudaMalloc(&d, sizeof(double)), "debug buffer");
+    ES_CUDA(es::dev_malloc(&d, sizeof(double)), "debug buffer");
     cudaError_t e = es::launch_debug_trace(L, ph, px, py, d, ctx->stream);
     if (e == cudaSuccess) ctx->launches++;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out_lifetime, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = es::copy_async(out_lifetime, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     cudaFree(d);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "es_debug_trace");
@@ -811,17 +811,17 @@ es_status es_debug_next_cell(es_ctx* ctx, double center_x, double center_y, doub
     if (!is || !in6 || !out6 || !out_available) return fail(ctx, ES_ERR_BAD_ARG, "null argument");
     double* d = nullptr;
     int* d_avail = nullptr;
-    ES_CUDA(cudaMalloc(&d, sizeof(double) * 12), "debug buffers");
-    cudaError_t e = cudaMalloc(&d_avail, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d, in6, sizeof(double) * 6, cudaMemcpyHostToDevice, ctx->stream);
+    ES_CUDA(es::dev_malloc(&d, sizeof(double) * 12), "debug buffers");
+    cudaError_t e = es::dev_malloc(&d_avail, sizeof(int));
+    if (e == cudaSuccess) e = es::copy_async(d, in6, sizeof(double) * 6, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
         e = es::launch_debug_next_cell(center_x, center_y, radius, clockwise, phi, is->spawn_region_start,
                                        is->spawn_region_size, is->cell_size, is->cells_per_row, d, d + 6, d_avail,
                                        ctx->stream);
     if (e == cudaSuccess) ctx->launches++;
     int avail = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out6, d + 6, sizeof(double) * 6, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&avail, d_avail, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = es::copy_async(out6, d + 6, sizeof(double) * 6, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = es::copy_async(&avail, d_avail, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     cudaFree(d);
     cudaFree(d_avail);

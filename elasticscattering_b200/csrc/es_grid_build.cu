@@ -27,6 +27,7 @@
 #include <cstdio>
 
 #include "es_cuda.h"
+#include "es_nvtx.h"
 #include "es_internal.h"
 
 struct es_dgrid {
@@ -340,13 +341,13 @@ es_status build(es_dgrid* g, uint32_t seed, double density, int32_t tcp, int64_t
 
     Scratch s;
     ES_DG_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "stream");
-    ES_DG_CUDA(cudaMalloc(&s.d_pos, sizeof(double2) * (size_t)n), "impurity positions");
-    ES_DG_CUDA(cudaMalloc(&s.d_count, sizeof(unsigned int) * (size_t)n_cells), "cell counts");
-    ES_DG_CUDA(cudaMalloc(&s.d_cursor, sizeof(unsigned int) * (size_t)n_cells), "cell cursors");
-    ES_DG_CUDA(cudaMalloc(&s.d_prefix, sizeof(unsigned long long) * (size_t)n_cells), "cell prefix");
-    ES_DG_CUDA(cudaMalloc(&s.d_tiles, sizeof(unsigned long long) * (size_t)n_tiles), "scan tiles");
-    ES_DG_CUDA(cudaMalloc(&s.d_total, sizeof(unsigned long long)), "scan total");
-    ES_DG_CUDA(cudaMalloc(&g->d_cell_end, sizeof(int) * (size_t)n_cells), "cell index");
+    ES_DG_CUDA(es::dev_malloc(&s.d_pos, sizeof(double2) * (size_t)n), "impurity positions");
+    ES_DG_CUDA(es::dev_malloc(&s.d_count, sizeof(unsigned int) * (size_t)n_cells), "cell counts");
+    ES_DG_CUDA(es::dev_malloc(&s.d_cursor, sizeof(unsigned int) * (size_t)n_cells), "cell cursors");
+    ES_DG_CUDA(es::dev_malloc(&s.d_prefix, sizeof(unsigned long long) * (size_t)n_cells), "cell prefix");
+    ES_DG_CUDA(es::dev_malloc(&s.d_tiles, sizeof(unsigned long long) * (size_t)n_tiles), "scan tiles");
+    ES_DG_CUDA(es::dev_malloc(&s.d_total, sizeof(unsigned long long)), "scan total");
+    ES_DG_CUDA(es::dev_malloc(&g->d_cell_end, sizeof(int) * (size_t)n_cells), "cell index");
 
     // GenerateImpurities (src/sim/Grid.cpp:61-75): the seed passes through an
     // int, and minstd_rand0 maps a zero state to 1.
@@ -354,34 +355,34 @@ es_status build(es_dgrid* g, uint32_t seed, double density, int32_t tcp, int64_t
     unsigned long long x0 = s64 % kMinstdM;
     if (x0 == 0) x0 = 1;
     generate_kernel<<<blocks_for(n, 256), 256, 0, s.stream>>>(x0, n, lo, hi, s.d_pos);
-    ES_DG_CUDA(cudaGetLastError(), "generate_kernel");
+    ES_DG_CUDA(es::launched(s.stream), "generate_kernel");
 
     // GenerateImpurityCells + ConvertToIndex (src/sim/Grid.cpp:77-110)
     const Geo geo{lo, hi - lo, g->is.cell_size, cpr};
     const double r = g->is.impurity_radius;
     ES_DG_CUDA(cudaMemsetAsync(s.d_count, 0, sizeof(unsigned int) * (size_t)n_cells, s.stream), "count clear");
     count_kernel<<<blocks_for(n, 256), 256, 0, s.stream>>>(s.d_pos, n, geo, r, s.d_count);
-    ES_DG_CUDA(cudaGetLastError(), "count_kernel");
+    ES_DG_CUDA(es::launched(s.stream), "count_kernel");
     scan_tiles_kernel<<<(unsigned)n_tiles, kScanThreads, 0, s.stream>>>(s.d_count, n_cells, s.d_prefix, s.d_tiles);
-    ES_DG_CUDA(cudaGetLastError(), "scan_tiles_kernel");
+    ES_DG_CUDA(es::launched(s.stream), "scan_tiles_kernel");
     scan_totals_kernel<<<1, kScanThreads, 0, s.stream>>>(s.d_tiles, n_tiles, s.d_total);
-    ES_DG_CUDA(cudaGetLastError(), "scan_totals_kernel");
+    ES_DG_CUDA(es::launched(s.stream), "scan_totals_kernel");
     unsigned long long total = 0;
-    ES_DG_CUDA(cudaMemcpyAsync(&total, s.d_total, sizeof total, cudaMemcpyDeviceToHost, s.stream), "scan total");
+    ES_DG_CUDA(es::copy_async(&total, s.d_total, sizeof total, cudaMemcpyDeviceToHost, s.stream), "scan total");
     ES_DG_CUDA(cudaStreamSynchronize(s.stream), "grid build");
     if (total > 0x7fffffffULL)
         return dgrid_fail(ES_ERR_BAD_ARG, "indexed impurity count %lld exceeds the int32 cell index", (long long)total);
     finish_scan_kernel<<<blocks_for(n_cells, 256), 256, 0, s.stream>>>(s.d_count, s.d_prefix, s.d_tiles, n_cells,
                                                                        s.d_cursor, g->d_cell_end);
-    ES_DG_CUDA(cudaGetLastError(), "finish_scan_kernel");
+    ES_DG_CUDA(es::launched(s.stream), "finish_scan_kernel");
     const size_t n_alloc = (size_t)(total > 0 ? total : 1);
-    ES_DG_CUDA(cudaMalloc(&s.d_idx, sizeof(int) * n_alloc), "placement index");
-    ES_DG_CUDA(cudaMalloc(&g->d_imps, sizeof(double2) * n_alloc), "ordered impurities");
+    ES_DG_CUDA(es::dev_malloc(&s.d_idx, sizeof(int) * n_alloc), "placement index");
+    ES_DG_CUDA(es::dev_malloc(&g->d_imps, sizeof(double2) * n_alloc), "ordered impurities");
     place_kernel<<<blocks_for(n, 256), 256, 0, s.stream>>>(s.d_pos, n, geo, r, s.d_cursor, s.d_idx);
-    ES_DG_CUDA(cudaGetLastError(), "place_kernel");
+    ES_DG_CUDA(es::launched(s.stream), "place_kernel");
     order_kernel<<<blocks_for(n_cells * 32, 256), 256, 0, s.stream>>>(s.d_pos, s.d_idx, g->d_cell_end, n_cells,
                                                                        g->d_imps);
-    ES_DG_CUDA(cudaGetLastError(), "order_kernel");
+    ES_DG_CUDA(es::launched(s.stream), "order_kernel");
     ES_DG_CUDA(cudaStreamSynchronize(s.stream), "grid build");
     g->n_indexed = (int64_t)total;
     return ES_OK;
@@ -395,6 +396,7 @@ es_status es_dgrid_create_seeded(int32_t device_ordinal, uint32_t seed, double r
                                  double density, double impurity_radius, int32_t target_cell_population,
                                  int64_t max_impurities, es_dgrid** out)
 {
+    es::Range nvtx_range("grid_build");
     if (!out) return dgrid_fail(ES_ERR_BAD_ARG, "es_dgrid_create_seeded: null output");
     *out = nullptr;
     if (target_cell_population < 1) return dgrid_fail(ES_ERR_BAD_ARG, "target_cell_population must be >= 1");
@@ -444,10 +446,10 @@ es_status es_dgrid_download(const es_dgrid* g, double* out_xy, int32_t* out_cell
     if (!g) return dgrid_fail(ES_ERR_BAD_ARG, "es_dgrid_download: null grid");
     ES_DG_CUDA(cudaSetDevice(g->device), "cudaSetDevice");
     if (out_xy && g->n_indexed > 0)
-        ES_DG_CUDA(cudaMemcpy(out_xy, g->d_imps, sizeof(double2) * (size_t)g->n_indexed, cudaMemcpyDeviceToHost),
+        ES_DG_CUDA(es::copy_sync(out_xy, g->d_imps, sizeof(double2) * (size_t)g->n_indexed, cudaMemcpyDeviceToHost),
                    "impurity download");
     if (out_cell_end)
-        ES_DG_CUDA(cudaMemcpy(out_cell_end, g->d_cell_end,
+        ES_DG_CUDA(es::copy_sync(out_cell_end, g->d_cell_end,
                               sizeof(int) * (size_t)g->is.cells_per_row * (size_t)g->is.cells_per_row,
                               cudaMemcpyDeviceToHost),
                    "cell index download");

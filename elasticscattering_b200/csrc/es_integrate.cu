@@ -418,11 +418,11 @@ cudaError_t launch_group(const IntegrateLaunch& L, cudaStream_t s)
         else
             integrate_flat_kernel<NT, false, kIntegrateThreads>
                 <<<L.n_blocks, kIntegrateThreads, sizeof(PhaseSigma) * L.n_phase, s>>>(L);
-        return cudaGetLastError();
+        return es::launched(s);
     }
     if (L.fp32) integrate_positions_kernel<NT, true, kThreads><<<L.n_blocks, kThreads, 0, s>>>(L);
     else integrate_positions_kernel<NT, false, kThreads><<<L.n_blocks, kThreads, 0, s>>>(L);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 }  // namespace
@@ -457,16 +457,16 @@ cudaError_t launch_integrate(const IntegrateLaunch& L0, cudaStream_t s)
     }
     if (e != cudaSuccess) return e;
     reduce_partials_kernel<<<1, 256, 0, s>>>(L);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 cudaError_t launch_lifetime_sum(const double* lifetimes, long long n, double* partial, double* out, cudaStream_t s)
 {
     lifetime_sum_kernel<<<kIntegrateBlocks, 256, 0, s>>>(lifetimes, n, partial);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = es::launched(s);
     if (e != cudaSuccess) return e;
     sum_partials_kernel<<<1, 256, 0, s>>>(partial, kIntegrateBlocks, out);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 }  // namespace es

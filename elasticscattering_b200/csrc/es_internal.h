@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "es_cuda.h"
+#include "es_fault.h"
 
 #include <cstdint>
 
@@ -73,12 +74,6 @@ struct LifetimeLaunch {
     // es_host_math.h): as kernel parameters they are constant-bank operands
     // instead of registers.
     float sc_r, sc_inv_r, sc_ir, sc_lo2, sc_hi2, sc_eps2, sc_band_d, sc_inv4r, sc_tangent_tol;
-    // Split kernel: lifetimes of an earlier pass over the same orbits (same grid,
-    // sector, start grid and phases; another field), indexed like `out`, or null.
-    // They predict each orbit's walk length; a block runs its orbits in the
-    // order of that prediction. Results do not depend on it.
-    const double* pred;
-    double pred_scale;            // particle speed / cell size: a lifetime -> cells travelled
 };
 
 // FP64 lifetime kernel choices (es_tuning.lifetime_variant). The values 1, 3,

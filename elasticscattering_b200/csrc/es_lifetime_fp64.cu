@@ -184,7 +184,7 @@ cudaError_t launch_debug_trace(const LifetimeLaunch& L, const PhaseOrbit& ph, do
                                cudaStream_t s)
 {
     debug_trace_kernel<<<1, 1, 0, s>>>(L, ph, px, py, d_out);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 namespace {
@@ -194,7 +194,7 @@ cudaError_t launch_per_thread(const LifetimeLaunch& L, cudaStream_t s)
 {
     const long long blocks = (L.n_orbits + 255) / 256;
     lifetime_fp64_kernel<kMinBlocks, kDefer><<<(unsigned)blocks, 256, 0, s>>>(L);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 }  // namespace
@@ -215,7 +215,7 @@ cudaError_t launch_debug_next_cell(double cx, double cy, double r, int clockwise
                                    int* d_avail, cudaStream_t s)
 {
     debug_next_cell_kernel<<<1, 1, 0, s>>>(cx, cy, r, clockwise, phi, start, size, cell, cpr, d_in6, d_out6, d_avail);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 }  // namespace es

@@ -11,60 +11,14 @@
 namespace es {
 namespace {
 
-constexpr int kCostBuckets = 16;  // predicted-walk classes; class kCostBuckets holds inactive slots
-
-// The orbit a thread of the block runs, in predicted-cost order (kSorted):
-// a lane's cost is its walk, and a warp waits for its longest walk, so a warp
-// of similar walks wastes fewer lane-steps. The prediction is the orbit's
-// lifetime in an earlier pass over the same orbits at another field (P.pred):
-// travelled cells = lifetime * v / L, bucketed as 3 log2(1 + 4 cells). The
-// order within the block is a stable counting sort on the bucket (warp peers by
-// __match_any_sync, then fixed-order offsets), so it is deterministic; every
-// orbit's arithmetic is unchanged, and its lifetime lands at its own index.
-// The block's 256 orbits are about half of one start position's phases, so the
-// warps keep their shared start cell (and broadcast disk loads).
-__device__ __forceinline__ int block_sorted_offset(const LifetimeLaunch& P)
-{
-    __shared__ unsigned s_off[kCostBuckets + 1][8];
-    __shared__ unsigned short s_slot[256];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long t = (long long)blockIdx.x * 256 + threadIdx.x;
-    int b = kCostBuckets;
-    if (t < P.n_orbits) {
-        const long long g = (long long)P.row0 * P.dim * P.n_phase + t;
-        const float cells = (float)(__ldg(P.pred + g) * P.pred_scale);
-        b = min(kCostBuckets - 1, max(0, __float2int_rd(3.0f * __log2f(1.0f + 4.0f * cells))));
-    }
-    const unsigned peers = __match_any_sync(0xffffffffu, b);
-    const unsigned rank = __popc(peers & ((1u << lane) - 1u));
-    for (int k = threadIdx.x; k < (kCostBuckets + 1) * 8; k += 256) (&s_off[0][0])[k] = 0u;
-    __syncthreads();
-    if (rank == 0) s_off[b][warp] = __popc(peers);
-    __syncthreads();
-    if (threadIdx.x == 0) {  // exclusive scan, bucket-major then warp: a fixed order
-        unsigned run = 0;
-        for (int c = 0; c <= kCostBuckets; c++)
-            for (int w = 0; w < 8; w++) {
-                const unsigned n = s_off[c][w];
-                s_off[c][w] = run;
-                run += n;
-            }
-    }
-    __syncthreads();
-    s_slot[s_off[b][warp] + rank] = (unsigned short)threadIdx.x;
-    __syncthreads();
-    return s_slot[threadIdx.x];
-}
-
 // kDefer: the winner's FP64 time after a warp sync (split_orbit_synced), for
 // passes whose walks end after differing numbers of cell steps; otherwise
 // inside the walk (split_orbit), for passes where nearly every walk ends in
 // its first cell, where the synced form only adds register pressure.
-// kSorted: the block runs its orbits in predicted-cost order (block_sorted_offset).
-template <int kMinBlocks, bool kDefer, bool kSorted>
+template <int kMinBlocks, bool kDefer>
 __global__ void __launch_bounds__(256, kMinBlocks) lifetime_split_kernel(LifetimeLaunch P)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + (kSorted ? block_sorted_offset(P) : threadIdx.x);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = t < P.n_orbits;
     const unsigned mask = __ballot_sync(0xffffffffu, active);
     if (!active) return;
@@ -139,19 +93,14 @@ cudaError_t launch_lifetimes_split(const LifetimeLaunch& L, bool defer_finish, c
     if (e != cudaSuccess) return e;
     if (L.orbit_table != nullptr) {
         orbit_table_kernel<<<(unsigned)((L.n_phase + 127) / 128), 128, 0, s>>>(L);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = es::launched(s)) != cudaSuccess) return e;
     }
     const long long blocks = (L.n_orbits + 255) / 256;
-    if (L.pred != nullptr) {
-        if (defer_finish) lifetime_split_kernel<4, true, true><<<(unsigned)blocks, 256, 0, s>>>(L);
-        else lifetime_split_kernel<4, false, true><<<(unsigned)blocks, 256, 0, s>>>(L);
-    } else {
-        if (defer_finish) lifetime_split_kernel<4, true, false><<<(unsigned)blocks, 256, 0, s>>>(L);
-        else lifetime_split_kernel<4, false, false><<<(unsigned)blocks, 256, 0, s>>>(L);
-    }
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (defer_finish) lifetime_split_kernel<4, true><<<(unsigned)blocks, 256, 0, s>>>(L);
+    else lifetime_split_kernel<4, false><<<(unsigned)blocks, 256, 0, s>>>(L);
+    if ((e = es::launched(s)) != cudaSuccess) return e;
     lifetime_retrace_kernel<<<148 * 4, 256, 0, s>>>(L);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 cudaError_t launch_local_impurities(const double2* imps, const int* cell_end, float2* out, double start, double cell,
@@ -159,7 +108,7 @@ cudaError_t launch_local_impurities(const double2* imps, const int* cell_end, fl
 {
     const long long n = (long long)cpr * cpr;
     local_impurities_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(imps, cell_end, out, start, cell, cpr);
-    return cudaGetLastError();
+    return es::launched(s);
 }
 
 }  // namespace es

@@ -18,6 +18,7 @@
 // on the caller's stream.
 #include "es_cuda.h"
 #include "es_host_math.h"
+#include "es_nvtx.h"
 #include "es_internal.h"
 
 #include <cuda.h>
@@ -138,6 +139,7 @@ extern "C" es_status es_derive_temperatures_noalloc(const double* d_lifetimes, i
                                                     double magnetic_field, const double* temperatures, int32_t n_t,
                                                     double* d_out_sigma, void* stream)
 {
+    es::Range nvtx_range("temperatures_noalloc");
     // Every argument is checked before anything is enqueued: an error return
     // means no work was queued and d_out_sigma is untouched.
     if (!d_lifetimes || !d_out_sigma || !s || (n_t > 0 && !temperatures) || n_t < 0)
@@ -172,7 +174,7 @@ extern "C" es_status es_derive_temperatures_noalloc(const double* d_lifetimes, i
     const es::host::Sector sec = es::host::sector(s->alpha, phi_steps, coherent != 0);
     const int n_phase = 4 * phi_steps;
     noalloc_phase_table_kernel<<<(n_phase + 127) / 128, 128, 0, cs>>>(table, phi_steps, sec.phi_start, sec.phi_step);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = es::launched(cs);
 
     // SimulationCPU::ComputeLifetimes, src/sim/SimulationCPU.cpp:107-108
     const double w = es::host::angular_speed(magnetic_field);

@@ -146,6 +146,7 @@ RunConfig ParseConfigText(const std::string& text, const std::string& file_path)
     }
     cfg.batched = has(values, "batched") && std::atoi(values.at("batched").c_str()) == 1;
     cfg.device_ordinal = has(values, "device_ordinal") ? std::atoi(values.at("device_ordinal").c_str()) : 0;
+    cfg.journal_path = has(values, "journal") ? values.at("journal") : "";
     return cfg;
 }
 
@@ -185,7 +186,7 @@ std::string DescribeConfig(const RunConfig& c)
       << ", \"target_cell_population\": " << c.settings.target_cell_population
       << ", \"output_directory\": \"" << c.output_directory << "\", \"digits_in_sample_num\": "
       << c.digits_in_sample_num << ", \"precision\": " << c.precision << ", \"batched\": " << (c.batched ? 1 : 0)
-      << ", \"device_ordinal\": " << c.device_ordinal << "}";
+      << ", \"device_ordinal\": " << c.device_ordinal << ", \"journal\": \"" << c.journal_path << "\"}";
     return o.str();
 }
 

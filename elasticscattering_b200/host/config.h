@@ -7,7 +7,8 @@
 //
 // Keys this build adds (ignored by the reference): `precision fp64|split`
 // (default fp64: the reference's arithmetic), `batched 0|1` (1: every sample,
-// field and sector in one batched run), `device_ordinal n`.
+// field and sector in one batched run), `device_ordinal n`, `journal <path>`
+// (the per-pass results journal that lets a stopped sweep resume; journal.h).
 #pragma once
 
 #include <cstdint>
@@ -45,6 +46,7 @@ struct RunConfig {
     int precision = ES_PRECISION_FP64;
     bool batched = false;
     int device_ordinal = 0;
+    std::string journal_path;  // empty: no journal
 };
 
 // Key/value lines as the reference reads them: empty lines and lines starting

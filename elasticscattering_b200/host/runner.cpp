@@ -8,6 +8,13 @@
 // field, sector) pass of the config in one batched graph replay instead and
 // writes the same files (without the per-position images, which the batched
 // path does not materialise).
+//
+// With `journal <path>` every finished pass is appended to the journal, and a
+// pass already there (same run inputs, sample seed, sector and field) is taken
+// from it instead of being computed (journal.h). A resumed pass writes no
+// per-position images: they are in the results folder of the run that
+// computed it. The device context of the per-pass mode is created at the first
+// pass to compute, so a sweep found whole in the journal needs no GPU.
 #include "runner.h"
 
 #include <chrono>
@@ -19,6 +26,7 @@
 #include <sstream>
 
 #include "es_host.h"
+#include "es_nvtx.h"
 #include "logger.h"
 
 void es_host_set_error(const char* msg);
@@ -44,8 +52,15 @@ SimulationResult SimulationRunner::Run(const std::string& config_path) { return 
 
 SimulationResult SimulationRunner::Run(const RunConfig& cfg)
 {
+    es::Range nvtx_range("sweep");
     cfg_ = cfg;
+    resumed_ = computed_ = 0;
+    journal_.reset();
     log_ << "Starting simulation (" << cfg_.config_path << ")" << std::endl;
+    if (!cfg_.journal_path.empty()) {
+        journal_ = std::make_unique<Journal>(cfg_.journal_path, cfg_);
+        log_ << "Journal: " << cfg_.journal_path << " (" << journal_->size() << " passes of this run)" << std::endl;
+    }
     if (cfg_.output_type != OutputType::Nothing) {
         log_ << "Output directory: " << cfg_.output_directory << std::endl;
         CreateOutputDirectory();
@@ -54,6 +69,7 @@ SimulationResult SimulationRunner::Run(const RunConfig& cfg)
     const double t0 = now_s();
     SimulationResult sr = cfg_.batched ? RunBatched() : RunSimulation();
     log_ << std::endl << "Finished! (" << (now_s() - t0) << "s)" << std::endl;
+    if (journal_) log_ << "Passes: " << computed_ << " computed, " << resumed_ << " from the journal" << std::endl;
     if (cfg_.output_type != OutputType::Nothing) FinishResults(sr);
     return sr;
 }
@@ -78,13 +94,13 @@ SimulationResult SimulationRunner::RunSimulation()
     gi.index_size = (int64_t)grid->GetIndex().size();
     gi.region_size = cfg_.settings.region_size;
     gi.region_extends = cfg_.settings.region_extends;
-    SimulationCUDA es(cfg_.positions_per_row, cfg_.particles_per_quadrant, gi, cfg_.device_ordinal, cfg_.precision);
+    std::unique_ptr<SimulationCUDA> es;  // created at the first pass to compute
 
     SimulationResult sr;
     for (int i = 0; i < cfg_.num_samples; i++) {
         if (cfg_.output_type == OutputType::All) CreateSampleOutputDirectory(i);
-        sr.coherent.push_back(RunSample(es, i, true, *grid));
-        sr.incoherent.push_back(RunSample(es, i, false, *grid));
+        sr.coherent.push_back(RunSample(es, gi, i, true, *grid));
+        sr.incoherent.push_back(RunSample(es, gi, i, false, *grid));
         if (cfg_.output_type == OutputType::All)
             Logger::LogSampleResults(SampleResultsPath(i), sr.coherent[(size_t)i], sr.incoherent[(size_t)i]);
         if (i + 1 < cfg_.num_samples) grid = std::make_unique<Grid>(make_grid(cfg_, i + 1));
@@ -92,13 +108,43 @@ SimulationResult SimulationRunner::RunSimulation()
     return sr;
 }
 
-SampleResult SimulationRunner::RunSample(SimulationCUDA& es, int sample_index, bool coherent, const Grid& grid)
+void SimulationRunner::Record(int sample_index, bool coherent, double field, const std::vector<Sigma>& sigma,
+                              const Metrics& m)
+{
+    computed_++;
+    if (!journal_) return;
+    JournalEntry e;
+    e.sample = sample_index;
+    e.seed = cfg_.sample_seeds[(size_t)sample_index];
+    e.coherent = coherent;
+    e.field = field;
+    e.sigma = sigma;
+    e.metrics = m;
+    journal_->Append(e);
+}
+
+SampleResult SimulationRunner::RunSample(std::unique_ptr<SimulationCUDA>& es, const GridInformation& gi,
+                                         int sample_index, bool coherent, const Grid& grid)
 {
     const int T = (int)cfg_.temperatures.size();
     const int N = (int)cfg_.magnetic_fields.size();
     SampleResult sr(T, N);
     const int64_t nlifetimes = (int64_t)cfg_.positions_per_row * cfg_.positions_per_row * 4 * cfg_.particles_per_quadrant;
-    es.InitSample(grid, cfg_.settings, coherent);
+    const std::string range = "sample " + std::to_string(sample_index) + (coherent ? " coherent" : " incoherent");
+    es::Range nvtx_range(range.c_str());
+    std::vector<const JournalEntry*> done((size_t)N, nullptr);
+    int n_done = 0;
+    if (journal_)
+        for (int i = 0; i < N; i++)
+            if ((done[(size_t)i] = journal_->Find(sample_index, cfg_.sample_seeds[(size_t)sample_index], coherent,
+                                                 cfg_.magnetic_fields[(size_t)i])) != nullptr)
+                n_done++;
+    if (n_done < N) {
+        if (!es)
+            es = std::make_unique<SimulationCUDA>(cfg_.positions_per_row, cfg_.particles_per_quadrant, gi,
+                                                  cfg_.device_ordinal, cfg_.precision);
+        es->InitSample(grid, cfg_.settings, coherent);
+    }
     SampleMetrics sm(sample_index, coherent, nlifetimes);
     sm.total_indexed_impurities = grid.GetTotalImpurityCount();
     sm.impurity_count = grid.GetUniqueImpurityCount();
@@ -113,15 +159,23 @@ SampleResult SimulationRunner::RunSample(SimulationCUDA& es, int sample_index, b
     }
     for (int i = 0; i < N; i++) {
         const double B = cfg_.magnetic_fields[(size_t)i];
+        if (const JournalEntry* d = done[(size_t)i]) {
+            sr.results[(size_t)i] = d->sigma;
+            sm.iteration_metrics.push_back(d->metrics);
+            resumed_++;
+            log_ << "j" << std::flush;
+            continue;
+        }
         if (cfg_.output_type != OutputType::All) {
-            sr.results[(size_t)i] = es.ComputeSigmas(B, cfg_.temperatures, grid, sm);
+            sr.results[(size_t)i] = es->ComputeSigmas(B, cfg_.temperatures, grid, sm);
         } else {
-            auto it = es.ComputeSigmasWithImages(B, cfg_.temperatures, grid, sm);
+            auto it = es->ComputeSigmasWithImages(B, cfg_.temperatures, grid, sm);
             for (int j = 0; j < T; j++) {
                 sr.results[(size_t)i][(size_t)j] = it[(size_t)j].result;
                 Logger::LogImages(ImagePath(j, i, sample_index, coherent), cfg_.positions_per_row, it[(size_t)j]);
             }
         }
+        Record(sample_index, coherent, B, sr.results[(size_t)i], sm.iteration_metrics.back());
         log_ << "x" << std::flush;
     }
     if (cfg_.output_type != OutputType::Nothing) Logger::LogSampleMetrics(MetricsPath(), sm);
@@ -130,6 +184,7 @@ SampleResult SimulationRunner::RunSample(SimulationCUDA& es, int sample_index, b
 
 SimulationResult SimulationRunner::RunBatched()
 {
+    es::Range nvtx_range("batched_sweep");
     const int S = cfg_.num_samples, N = (int)cfg_.magnetic_fields.size(), T = (int)cfg_.temperatures.size();
     if (T > ES_BATCH_MAX_T) throw SimulationError("batched runs take at most 8 temperatures");
     es_batch* b = nullptr;
@@ -180,9 +235,18 @@ SimulationResult SimulationRunner::RunBatched()
     // for every sample (src/SimulationRunner.cpp:76-86).
     const double cell0 = grids[0].is.cell_size;
     std::vector<es_batch_instance> inst;
+    // per (sample, sector, field): the journal's entry, or the batch instance
+    std::vector<const JournalEntry*> done;
+    std::vector<size_t> slot;
     for (int s = 0; s < S; s++)
         for (int coh = 1; coh >= 0; coh--)
             for (int i = 0; i < N; i++) {
+                const JournalEntry* d =
+                    journal_ ? journal_->Find(s, cfg_.sample_seeds[(size_t)s], coh == 1, cfg_.magnetic_fields[(size_t)i])
+                             : nullptr;
+                done.push_back(d);
+                slot.push_back(inst.size());
+                if (d) continue;
                 es_batch_instance x{};
                 x.grid = ids[(size_t)s];
                 x.positions_per_row = cfg_.positions_per_row;
@@ -196,12 +260,15 @@ SimulationResult SimulationRunner::RunBatched()
                 for (int t = 0; t < T; t++) x.temperatures[t] = cfg_.temperatures[(size_t)t];
                 inst.push_back(x);
             }
-    check(es_batch_set_instances(b, inst.data(), (int32_t)inst.size()));
     std::vector<double> out(inst.size() * ES_BATCH_MAX_T * 2);
     std::vector<es_metrics> mets(inst.size());
-    const double t0 = now_s();
-    check(es_batch_run(b, out.data(), mets.data()));
-    const double run_s = now_s() - t0;
+    double run_s = 0;
+    if (!inst.empty()) {
+        check(es_batch_set_instances(b, inst.data(), (int32_t)inst.size()));
+        const double t0 = now_s();
+        check(es_batch_run(b, out.data(), mets.data()));
+        run_s = now_s() - t0;
+    }
     log_ << "Batched run: " << inst.size() << " passes in " << run_s << "s" << std::endl;
 
     SimulationResult sr;
@@ -217,14 +284,22 @@ SimulationResult SimulationRunner::RunBatched()
             sm.total_cells = (int64_t)g.is.cells_per_row * g.is.cells_per_row;
             sm.seed = g.seed;
             for (int i = 0; i < N; i++, k++) {
+                if (const JournalEntry* d = done[k]) {
+                    res.results[(size_t)i] = d->sigma;
+                    sm.iteration_metrics.push_back(d->metrics);
+                    resumed_++;
+                    continue;
+                }
+                const size_t q = slot[k];
                 for (int t = 0; t < T; t++)
-                    res.results[(size_t)i][(size_t)t] = Sigma(out[(k * ES_BATCH_MAX_T + t) * 2],
-                                                              out[(k * ES_BATCH_MAX_T + t) * 2 + 1]);
+                    res.results[(size_t)i][(size_t)t] = Sigma(out[(q * ES_BATCH_MAX_T + t) * 2],
+                                                              out[(q * ES_BATCH_MAX_T + t) * 2 + 1]);
                 Metrics m;
-                m.particle_metrics = mets[k];
-                m.real_particles = nlt - mets[k].particles_inside_impurity;
+                m.particle_metrics = mets[q];
+                m.real_particles = nlt - mets[q].particles_inside_impurity;
                 m.time_elapsed_lifetimes = run_s / (double)inst.size();  // the batch's mean time per pass
                 sm.iteration_metrics.push_back(m);
+                Record(s, coh == 1, cfg_.magnetic_fields[(size_t)i], res.results[(size_t)i], m);
             }
             if (cfg_.output_type != OutputType::Nothing) Logger::LogSampleMetrics(MetricsPath(), sm);
             (coh ? sr.coherent : sr.incoherent).push_back(res);

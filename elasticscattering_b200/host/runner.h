@@ -2,11 +2,13 @@
 // samples, magnetic fields and temperatures, with the reference's results folder.
 #pragma once
 
+#include <memory>
 #include <ostream>
 #include <string>
 #include <vector>
 
 #include "config.h"
+#include "journal.h"
 #include "simulation_cuda.h"
 
 namespace es_host {
@@ -23,11 +25,16 @@ public:
     SimulationResult Run(const std::string& config_path);
     SimulationResult Run(const RunConfig& cfg);
     const RunConfig& config() const { return cfg_; }
+    // Passes of the last Run taken from the journal / computed.
+    int64_t resumed_passes() const { return resumed_; }
+    int64_t computed_passes() const { return computed_; }
 
 private:
     SimulationResult RunSimulation();
     SimulationResult RunBatched();
-    SampleResult RunSample(SimulationCUDA& es, int sample_index, bool coherent, const Grid& grid);
+    SampleResult RunSample(std::unique_ptr<SimulationCUDA>& es, const GridInformation& gi, int sample_index,
+                           bool coherent, const Grid& grid);
+    void Record(int sample_index, bool coherent, double field, const std::vector<Sigma>& sigma, const Metrics& m);
     void FinishResults(const SimulationResult& sr) const;
     void CreateOutputDirectory() const;
     void CreateSampleOutputDirectory(int sample_index) const;
@@ -44,6 +51,8 @@ private:
 
     RunConfig cfg_;
     std::ostream& log_;
+    std::unique_ptr<Journal> journal_;
+    int64_t resumed_ = 0, computed_ = 0;
 };
 
 }  // namespace es_host

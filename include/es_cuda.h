@@ -428,6 +428,34 @@ es_status es_mlp_predict(es_mlp* m, const float* x, int64_t q, float* out_each, 
 int64_t es_mlp_launch_count(const es_mlp* m);
 void* es_mlp_stream(es_mlp* m);
 
+/* ---------------------------------------------------------------------------
+ * Host-side fault injection, for testing callers' error handling. No
+ * reference counterpart (the reference prints and exits on every error,
+ * src/utils/ErrorMacros.h:22-38).
+ *
+ * spec: comma-separated items "kind:N" or "kind:N+", kind one of
+ *   alloc   device and pinned-host allocations,
+ *   copy    host<->device and device<->device copies,
+ *   launch  kernel launches,
+ * made by the lifetime, integration, batch, grid-build and no-alloc entry
+ * points (the es_mlp_* surrogate calls are not counted). "kind:N" fails the
+ * N-th such operation (1-based, counted from this call) once; "kind:N+" fails
+ * the N-th and every later one. NULL or "" disarms. The environment variable
+ * ES_FAULT_INJECT arms the same syntax at the first counted operation, unless
+ * es_fault_inject was called first.
+ *
+ * An injected allocation failure makes nothing and returns ES_ERR_OOM. An
+ * injected copy or launch failure is reported (ES_ERR_LAUNCH) after the real
+ * operation was issued and its stream waited on, so memory holds what an
+ * error-free call would have written and nothing is left in flight; no GPU
+ * fault is ever provoked. After any failure the object stays usable: the call
+ * can be repeated (a context whose es_upload_grid or es_init_sample failed
+ * needs that call again first). */
+es_status es_fault_inject(const char* spec);
+/* Operations counted since the last es_fault_inject: out_counts[0] alloc,
+ * [1] copy, [2] launch, [3] how many were failed. */
+es_status es_fault_counts(int64_t* out_counts);
+
 /* Measured FP64 FMA throughput of a device (TFLOP/s, 2 FLOP per FMA): the
  * denominator of the lifetime kernel's roofline. No reference counterpart
  * (the reference publishes no device figures). Runs for a few milliseconds. */

@@ -152,3 +152,79 @@ def test_second_run_takes_the_next_result_folder(tmp_path, cuda_device):
     second = run_config(cfg)
     assert second.name == "Result_1"
     assert (second / "T0.dat").exists() and not (second / "Sample 0").exists()
+
+
+CLI = Path(__file__).resolve().parent.parent / "elasticscattering_b200" / "es_b200"
+TOTAL_PASSES = 2 * 2 * len(FIELDS)  # samples x sectors x fields
+
+
+def run_cli(cfg: Path, fault: str | None = None):
+    import os
+    import subprocess
+
+    env = dict(os.environ)
+    env.pop("ES_FAULT_INJECT", None)
+    if fault:
+        env["ES_FAULT_INJECT"] = fault
+    return subprocess.run([str(CLI), str(cfg)], capture_output=True, text=True, env=env, timeout=600)
+
+
+def pass_counts(stdout: str):
+    import re
+
+    m = re.search(r"Passes: (\d+) computed, (\d+) from the journal", stdout)
+    assert m, stdout
+    return int(m.group(1)), int(m.group(2))
+
+
+def result_rows(out: Path):
+    return [read_result_file(out / f"T{j}.dat") for j in range(len(TEMPS))]
+
+
+@pytest.mark.parametrize("extra", ["", "precision split\n"])
+def test_sweep_stopped_by_a_failure_resumes_from_the_journal(tmp_path, cuda_device, extra):
+    """A sweep stopped part way by an injected launch failure (ES_FAULT_INJECT,
+    host-side) exits non-zero with the error; run again with the same journal it
+    computes only the passes it had not finished, and its result files equal an
+    uninterrupted run's."""
+    from elasticscattering_b200 import journal
+
+    clean = tmp_path / "clean.config"
+    clean.write_text(config_text(tmp_path / "clean", "output_type results\n" + extra))
+    ref = result_rows(run_config(clean))
+
+    cfg = tmp_path / "sweep.config"
+    jpath = tmp_path / "sweep.jsonl"
+    cfg.write_text(config_text(tmp_path / "out", f"output_type results\njournal {jpath}\n" + extra))
+    r = run_cli(cfg, fault="launch:12+")
+    assert r.returncode != 0 and "launch" in r.stderr.lower(), (r.returncode, r.stderr)
+    done = len(journal.read(jpath))
+    assert 0 < done < TOTAL_PASSES, done
+
+    r = run_cli(cfg)
+    assert r.returncode == 0, r.stderr
+    assert pass_counts(r.stdout) == (TOTAL_PASSES - done, done)
+    assert len(journal.read(jpath)) == TOTAL_PASSES
+    got = result_rows(sorted((tmp_path / "out").glob("Result_*"))[-1])
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
+
+
+def test_batched_sweep_computes_only_the_passes_missing_from_the_journal(tmp_path, cuda_device):
+    from elasticscattering_b200 import journal
+
+    cfg = tmp_path / "sweep.config"
+    jpath = tmp_path / "sweep.jsonl"
+    cfg.write_text(config_text(tmp_path / "out", f"output_type results\nbatched 1\nprecision split\njournal {jpath}\n"))
+    r = run_cli(cfg)
+    assert r.returncode == 0, r.stderr
+    assert pass_counts(r.stdout) == (TOTAL_PASSES, 0)
+    first = result_rows(tmp_path / "out" / "Result_0")
+    lines = jpath.read_text().splitlines()
+    jpath.write_text("\n".join(lines[:2] + lines[5:]) + "\n")  # three passes lost
+    r = run_cli(cfg)
+    assert r.returncode == 0, r.stderr
+    assert pass_counts(r.stdout) == (3, TOTAL_PASSES - 3)
+    assert len(journal.read(jpath)) == TOTAL_PASSES
+    for a, b in zip(result_rows(tmp_path / "out" / "Result_1"), first):
+        assert np.array_equal(a, b)

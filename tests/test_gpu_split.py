@@ -164,33 +164,3 @@ def test_split_images_and_fp32_integration(cuda_device):
         plain.close()
         split.close()
 
-
-def test_walk_length_prediction_changes_no_result(cuda_device):
-    """A split context orders each block's orbits by the previous pass's lifetimes
-    (the same orbits at another field). The order is scheduling only: a pass run
-    after another field gives the same lifetimes, counters and sigma, bit for bit,
-    as the same pass run first in a fresh context."""
-    w = workloads.config1()
-    dim = 65
-    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
-                       w.target_cell_population)
-    s = make_settings(w.tau, w.alpha, w.clockwise, w.particle_speed, w.region_size, w.region_extends, w.density,
-                      w.impurity_radius, w.target_cell_population)
-    for coh in (True, False):
-        with SimulationCUDA(dim, w.phi_steps, g.info(), device=cuda_device, precision=N.ES_PRECISION_SPLIT) as a:
-            a.InitSample(g, s, coh)
-            lt_a, m_a = a.ComputeLifetimes(20.0)
-            sig_a = a.DeriveTemperatures([1e-3, 10.0])
-        with SimulationCUDA(dim, w.phi_steps, g.info(), device=cuda_device, precision=N.ES_PRECISION_SPLIT) as b:
-            b.InitSample(g, s, coh)
-            b.ComputeLifetimes(18.7)        # the prediction for the next pass
-            lt_b, m_b = b.ComputeLifetimes(20.0)
-            sig_b = b.DeriveTemperatures([1e-3, 10.0])
-            lt_c, m_c = b.ComputeLifetimes(5.0)   # a farther field, predicted by 20 T
-        assert np.array_equal(lt_a.view(np.int64), lt_b.view(np.int64))
-        assert m_a == m_b
-        assert [(x.xx, x.xy) for x in sig_a] == [(x.xx, x.xy) for x in sig_b]
-        with SimulationCUDA(dim, w.phi_steps, g.info(), device=cuda_device, precision=N.ES_PRECISION_SPLIT) as c:
-            c.InitSample(g, s, coh)
-            lt_d, m_d = c.ComputeLifetimes(5.0)
-        assert np.array_equal(lt_c.view(np.int64), lt_d.view(np.int64)) and m_c == m_d

@@ -135,3 +135,29 @@ def test_no_device_fails_loudly():
     with pytest.raises(EsError) as e:
         SimulationCUDA(65, 7, info)
     assert e.value.status == 5 and "device" in str(e.value).lower()
+
+
+def test_fault_injection_plan_syntax():
+    """es_fault_inject accepts "alloc|copy|launch:N[+]" items and rejects
+    anything else without touching the armed plan; the counters start at zero
+    with each call. No device is needed: the plan lives on the host."""
+    for spec in ("alloc:1", "copy:3,launch:2+", " launch:10 , alloc:2+ ", "", None):
+        _native.fault_inject(spec)
+        assert _native.fault_counts() == {"alloc": 0, "copy": 0, "launch": 0, "failed": 0}
+    for bad in ("alloc", "alloc:0", "alloc:-1", "free:1", "copy:x", "launch:1++", "copy:1,bogus"):
+        with pytest.raises(EsError) as e:
+            _native.fault_inject(bad)
+        assert e.value.status == 1
+    _native.fault_inject(None)
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-device error path")
+def test_fault_injection_counts_nothing_without_a_device():
+    """Argument and device checks come before the first counted operation."""
+    _native.fault_inject("alloc:1")
+    info = GridInformation(1e-6, 1e-7, 5e-8, 100, 100)
+    with pytest.raises(EsError) as e:
+        SimulationCUDA(65, 7, info)
+    assert e.value.status == 5
+    assert _native.fault_counts()["alloc"] == 0
+    _native.fault_inject(None)
