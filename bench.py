@@ -1039,6 +1039,24 @@ def run_surrogate(args) -> None:
 
     stated = serve(0.01)
     calibrated = serve(tol)
+
+    # one query at a time: the network pass (features, copies, kernels, untarget)
+    # against the simulator on that one query (its graph recorded and run for it)
+    sur.tolerance = 0.01
+    one_nn, one_sim = [], []
+    for k in range(3):
+        sur.query(judge_q[k:k + 1])
+    for k in range(64):
+        one_nn.append(1e3 * sur.query(judge_q[k:k + 1])[3]["network_s"])
+    sim(judge_q[:1])
+    for k in range(8):
+        t0 = time.perf_counter()
+        sim(judge_q[k:k + 1])
+        one_sim.append(1e3 * (time.perf_counter() - t0))
+    single = {"network_ms_median": statistics.median(one_nn), "simulator_ms_median": statistics.median(one_sim),
+              "latency_gain_median": statistics.median(one_sim) / statistics.median(one_nn),
+              "note": "a single query per call: the network pass alone (it answers at the stated spread) "
+                      "against the simulator run for that query"}
     line = {
         "metric": "sigma queries/sec (surrogate with fallback)", "value": stated["queries_per_sec"],
         "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -1052,6 +1070,7 @@ def run_surrogate(args) -> None:
                    "error_target": "1% at the 95th percentile of network answers, fallback at 1% member spread"},
         "operating_point_spread_1pct": stated,
         "operating_point_calibrated": calibrated,
+        "single_query_latency": single,
         "simulator_latency_ms_per_query": sim_ms_per_query,
         "simulator_latency_ms_per_batch_extrapolated": sim_ms_per_query * Q,
         "network_only_error": {"queries": int(len(judge_q)), "p50": float(np.median(nn_only)),

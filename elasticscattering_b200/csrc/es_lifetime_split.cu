@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) lifetime_split_kernel(Lifetim
     int flags;
     double lt;
     const bool retrace = kDefer ? split_orbit_synced(LaunchFields{P}, g, mask, cnt, flags, lt)
-                                : split_orbit(LaunchFields{P}, g, cnt, flags, lt);
+                                : split_orbit(LaunchFields{P}, g, cnt, flags, lt, mask);
     if (retrace) {
         const unsigned long long slot = atomicAdd(P.retrace_count, 1ull);
         if (slot < (unsigned long long)P.retrace_cap) P.retrace[slot] = g;

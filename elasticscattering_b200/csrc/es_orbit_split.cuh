@@ -263,6 +263,77 @@ struct SplitCounters {
     int cells, imps, crossings, start_tests;
 };
 
+// The start-cell InsideImpurity scan (lifetime.h:90-99): the disks tested (up
+// to and including the first that holds the start) and whether one does.
+// tests < 0: not yet scanned.
+struct StartScan {
+    int tests;
+    bool inside;
+};
+
+// One disk of the scan: FP32 d^2 against r_i^2, decided in FP64 within a
+// relative 1e-4 band of the edge.
+template <class F>
+__device__ __forceinline__ bool start_inside(const F& f, dv2 pos, float plx, float ply, float ir2, int k)
+{
+    const float2 q = __ldg(f.imps32() + k);
+    const float dx = plx - q.x, dy = ply - q.y;
+    const float d2 = fmaf(dx, dx, dy * dy);
+    bool inside = d2 < ir2;
+    if (fabsf(d2 - ir2) <= 1e-4f * ir2) {
+        const double2 q64 = __ldg(f.imps() + k);
+        inside = inside_impurity(pos, dv2{q64.x, q64.y}, f.imp_radius());
+    }
+    return inside;
+}
+
+// The scan by one lane: the disks of the start cell in order.
+template <class F>
+__device__ __forceinline__ StartScan start_scan_lane(const F& f, dv2 pos, int cx, int cy)
+{
+    const int c = cy * f.cpr() + cx;
+    const int k0 = (c == 0) ? 0 : __ldg(f.cell_end() + c - 1);
+    const int k1 = __ldg(f.cell_end() + c);
+    const float plx = (float)(pos.x - (f.spawn_start() + cx * f.cell_size()));
+    const float ply = (float)(pos.y - (f.spawn_start() + cy * f.cell_size()));
+    const float ir = f.ir32();
+    const float ir2 = ir * ir;
+    for (int k = k0; k < k1; k++)
+        if (start_inside(f, pos, plx, ply, ir2, k)) return StartScan{k - k0 + 1, true};
+    return StartScan{k1 - k0, false};
+}
+
+// The same scan shared by the lanes of `mask`, which all start at `pos` (the
+// phases of one start position): the lane of rank r tests disks k0 + r,
+// k0 + r + n, ... (n lanes), and a ballot per round finds the first disk that
+// holds the start. Each disk's test is start_inside, so the decision and the
+// count are the per-lane scan's; the scan takes ceil(disks / n) rounds instead
+// of one round per disk.
+template <class F>
+__device__ __forceinline__ StartScan start_scan_shared(const F& f, dv2 pos, int cx, int cy, unsigned mask)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const int rank = __popc(mask & ((1u << lane) - 1u));
+    const int n = __popc(mask);
+    const int c = cy * f.cpr() + cx;
+    const int k0 = (c == 0) ? 0 : __ldg(f.cell_end() + c - 1);
+    const int k1 = __ldg(f.cell_end() + c);
+    const float plx = (float)(pos.x - (f.spawn_start() + cx * f.cell_size()));
+    const float ply = (float)(pos.y - (f.spawn_start() + cy * f.cell_size()));
+    const float ir = f.ir32();
+    const float ir2 = ir * ir;
+    for (int base = k0; base < k1; base += n) {  // the same trip count on every lane of mask
+        const int k = base + rank;
+        const bool inside = k < k1 && start_inside(f, pos, plx, ply, ir2, k);
+        const unsigned hit = __ballot_sync(mask, inside);
+        if (hit) {
+            const int first = __popc(mask & ((1u << (__ffs(hit) - 1)) - 1u));
+            return StartScan{base - k0 + first + 1, true};
+        }
+    }
+    return StartScan{k1 - k0, false};
+}
+
 // kSplitHit: the walk found its winning disk (and a near-equal runner-up);
 // the FP64 time of the crossing is still to be computed (finish_hit).
 enum SplitOutcome : int { kSplitDone = 0, kSplitRetrace = 1, kSplitHit = 2 };
@@ -293,7 +364,7 @@ __device__ __forceinline__ double finish_hit(const F& f, const OrbitD& o, int wi
 // finish_hit.
 template <class F, bool kDefer = false>
 __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos, SplitCounters& cnt, int& flags,
-                                           double& out, int2& win)
+                                           double& out, int2& win, StartScan start = StartScan{-1, false})
 {
     const double r64 = o.radius;
     // The pass's FP32 constants (split_constants, es_host_math.h): r, 1/r, r_i;
@@ -316,30 +387,14 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
     int cx = (int)((pos.x - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
     int cy = (int)((pos.y - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
 
-    // Start-cell InsideImpurity scan (lifetime.h:90-99), FP32 with an FP64 band.
-    {
-        const int c = cy * f.cpr() + cx;
-        const int k0 = (c == 0) ? 0 : __ldg(f.cell_end() + c - 1);
-        const int k1 = __ldg(f.cell_end() + c);
-        const float plx = (float)(pos.x - (f.spawn_start() + cx * f.cell_size()));
-        const float ply = (float)(pos.y - (f.spawn_start() + cy * f.cell_size()));
-        const float ir2 = ir * ir;
-        for (int k = k0; k < k1; k++) {
-            const float2 q = __ldg(f.imps32() + k);
-            const float dx = plx - q.x, dy = ply - q.y;
-            const float d2 = fmaf(dx, dx, dy * dy);
-            cnt.start_tests += 1;
-            bool inside = d2 < ir2;
-            if (fabsf(d2 - ir2) <= 1e-4f * ir2) {
-                const double2 q64 = __ldg(f.imps() + k);
-                inside = inside_impurity(pos, dv2{q64.x, q64.y}, f.imp_radius());
-            }
-            if (inside) {
-                flags = kTraceInside;
-                out = 0.0;
-                return kSplitDone;
-            }
-        }
+    // Start-cell InsideImpurity scan (lifetime.h:90-99), FP32 with an FP64 band,
+    // unless the caller's lanes shared it (start_scan_shared).
+    if (start.tests < 0) start = start_scan_lane(f, pos, cx, cy);
+    cnt.start_tests += start.tests;
+    if (start.inside) {
+        flags = kTraceInside;
+        out = 0.0;
+        return kSplitDone;
     }
 
     // Crossing advances of the current cell's four edge lines (x-lo, x-hi,
@@ -692,10 +747,27 @@ __device__ __forceinline__ OrbitD make_orbit(const LifetimeLaunch& P, long long 
     return make_orbit(LaunchFields{P}, g, pos);
 }
 
+// The start scan of the lanes of `mask` (0: none), shared when they all start
+// at the same position inside the grid, else left to each lane (tests < 0).
+// Every lane of a nonzero mask calls this.
+template <class F>
+__device__ __forceinline__ StartScan warp_start_scan(const F& f, dv2 pos, int cx, int cy, bool in_grid,
+                                                     unsigned mask)
+{
+    if (mask == 0u) return StartScan{-1, false};
+    const int src = __ffs(mask) - 1;
+    const double x0 = __shfl_sync(mask, pos.x, src), y0 = __shfl_sync(mask, pos.y, src);
+    if (!__all_sync(mask, pos.x == x0 && pos.y == y0 && in_grid)) return StartScan{-1, false};
+    return start_scan_shared(f, pos, cx, cy, mask);
+}
+
 // The split walk of orbit g. Returns true when the orbit must be re-traced in
 // FP64 (cnt and flags are then cleared); otherwise lt holds its lifetime.
+// `mask`: the warp's lanes that call this together (their start scan is
+// shared when they start at one position), or 0.
 template <class F>
-__device__ __forceinline__ bool split_orbit(const F& f, long long g, SplitCounters& cnt, int& flags, double& lt)
+__device__ __forceinline__ bool split_orbit(const F& f, long long g, SplitCounters& cnt, int& flags, double& lt,
+                                            unsigned mask = 0u)
 {
     dv2 pos;
     const OrbitD o = make_orbit(f, g, pos);
@@ -704,12 +776,14 @@ __device__ __forceinline__ bool split_orbit(const F& f, long long g, SplitCounte
     lt = 0.0;
     const int cx = (int)((pos.x - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
     const int cy = (int)((pos.y - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
-    if (cx < 0 || cy < 0 || cx >= f.cpr() || cy >= f.cpr()) {
+    const bool in_grid = !(cx < 0 || cy < 0 || cx >= f.cpr() || cy >= f.cpr());
+    const StartScan start = warp_start_scan(f, pos, cx, cy, in_grid, mask);
+    if (!in_grid) {
         atomicOr(f.error(), kErrStartCell);
         return false;
     }
     int2 win;
-    if (trace_split(f, o, pos, cnt, flags, lt, win) == kSplitRetrace) {
+    if (trace_split(f, o, pos, cnt, flags, lt, win, start) == kSplitRetrace) {
         cnt = SplitCounters{0, 0, 0, 0};
         flags = kTraceOk;
         return true;
@@ -740,8 +814,10 @@ __device__ __forceinline__ bool split_orbit_synced(const F& f, long long g, unsi
     int2 win = make_int2(-1, -1);
     const int cx = (int)((pos.x - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
     const int cy = (int)((pos.y - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
-    if (cx < 0 || cy < 0 || cx >= f.cpr() || cy >= f.cpr()) atomicOr(f.error(), kErrStartCell);
-    else st = trace_split<F, true>(f, o, pos, cnt, flags, lt, win);
+    const bool in_grid = !(cx < 0 || cy < 0 || cx >= f.cpr() || cy >= f.cpr());
+    const StartScan start = warp_start_scan(f, pos, cx, cy, in_grid, mask);
+    if (!in_grid) atomicOr(f.error(), kErrStartCell);
+    else st = trace_split<F, true>(f, o, pos, cnt, flags, lt, win, start);
     __syncwarp(mask);
     if (st == kSplitHit) {
         lt = finish_hit(f, o, win.x, win.y, flags);

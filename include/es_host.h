@@ -55,7 +55,11 @@ uint64_t es_grid_generation(const es_grid* g);
  * T<j>.dat, Metrics.txt and Sample <i>/ with sample_results.dat and the PNG
  * maps). The folder used is copied to out_directory (out_len bytes, may be
  * NULL). quiet != 0 suppresses the progress output. Errors, including config
- * errors the reference exits on, return non-OK with es_host_last_error(). */
+ * errors the reference exits on, return non-OK with es_host_last_error().
+ * With the added key `journal <path>` every finished (sample, sector, field)
+ * pass is appended to that file as one JSON line, and passes already there
+ * (same run inputs) are taken from it instead of being computed, so a stopped
+ * sweep resumes; a sweep found whole in the journal makes no device call. */
 es_status es_run_config(const char* config_path, char* out_directory, int32_t out_len, int32_t quiet);
 
 /* The parsed form of a .config file (the values es_run_config would use) as a

@@ -72,7 +72,7 @@ def steps_pass():
 
     def images(s):
         its = s["sim"].ComputeSigmasWithImages(40.0, TEMPS)
-        return np.concatenate([np.concatenate([it.lifetime, it.xx, it.xy, [it.result.xx, it.result.xy]])
+        return np.concatenate([np.concatenate([it.particle_lifetimes, it.xx_buffer, it.xy_buffer, [it.result.xx, it.result.xy]])
                                for it in its])
 
     def lifetimes(s):
