@@ -224,7 +224,8 @@ __global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks) batch_kernel(Bat
         for (int it = 0; it < B.chunk_iters; it++) {
             const long long g = g0 + (long long)it * 32 + lane;
             const bool active = g < I.L.n_orbits;
-            if (!__any_sync(0xffffffffu, active)) break;
+            const unsigned amask = __ballot_sync(0xffffffffu, active);
+            if (amask == 0u) break;
             unsigned cells = 0, imps = 0, cross = 0, starts = 0;
             int flags = kTraceOk;
             bool retrace = false;
@@ -232,7 +233,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32, kMinBlocks) batch_kernel(Bat
                 double lt = 0.0;
                 if (kPrec == ES_PRECISION_SPLIT) {
                     SplitCounters sc;
-                    retrace = split_orbit(SharedFields{&I.L}, g, sc, flags, lt);
+                    retrace = split_orbit(SharedFields{&I.L}, g, sc, flags, lt, amask);
                     cells = sc.cells, imps = sc.imps, cross = sc.crossings, starts = sc.start_tests;
                 } else {
                     OrbitCounters oc;

@@ -104,10 +104,20 @@ __global__ void __launch_bounds__(256, kMinBlocks) lifetime_fp64_kernel(Lifetime
     int flags = kTraceOk;
     double lt = 0.0;
     const iv2 c0 = get_cell(position, gr.start, gr.size, gr.cpr);
-    if (!within_bounds(c0, gr.cpr)) {
+    const bool in_grid = within_bounds(c0, gr.cpr);
+    // The start-cell scan depends on the start position only: when the warp's
+    // lanes all start at one position, they share it.
+    StartScan start{-1, false};
+    {
+        const int src = __ffs(mask) - 1;
+        const long long p0 = __shfl_sync(mask, pidx, src);
+        if (__all_sync(mask, pidx == p0 && in_grid))
+            start = start_scan_shared64(gr.imps, gr.cell_end, c0.y * gr.cpr + c0.x, position, gr.imp_r, mask);
+    }
+    if (!in_grid) {
         atomicOr(P.error, kErrStartCell);
     } else {
-        lt = trace_orbit<kDefer>(o, position, ph.phi, P.w, gr, P.walk_cap, cnt, flags, s_defer + threadIdx.x);
+        lt = trace_orbit<kDefer>(o, position, ph.phi, P.w, gr, P.walk_cap, cnt, flags, s_defer + threadIdx.x, start);
         if (flags & kTraceWalkCap) atomicOr(P.error, kErrWalkCap);
     }
     P.out[g] = lt;

@@ -262,6 +262,43 @@ __device__ __forceinline__ bool next_cell(const OrbitD& o, double phi, const Gri
            !angle_in_range(phi, last.incident_angle, next.incident_angle, o.clockwise);
 }
 
+// The start-cell InsideImpurity scan (lifetime.h:90-99): the disks tested (up
+// to and including the first that holds the start) and whether one does.
+// tests < 0: not yet scanned.
+struct StartScan {
+    int tests;
+    bool inside;
+};
+
+// The FP64 scan shared by the lanes of `mask`, which all start at `position`
+// in cell `pci` (the phases of one start position): the lane of rank r tests
+// disks k0 + r, k0 + r + n, ... (n lanes), and a ballot per round finds the
+// first disk that holds the start. Each test is InsideImpurity on the same
+// operands as the per-lane scan, so the decision and the count are its own.
+__device__ __forceinline__ StartScan start_scan_shared64(const double2* imps, const int* cell_end, int pci,
+                                                         dv2 position, double imp_r, unsigned mask)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const int rank = __popc(mask & ((1u << lane) - 1u));
+    const int n = __popc(mask);
+    const int k0 = (pci == 0) ? 0 : __ldg(cell_end + pci - 1);
+    const int k1 = __ldg(cell_end + pci);
+    for (int base = k0; base < k1; base += n) {  // the same trip count on every lane of mask
+        const int k = base + rank;
+        bool inside = false;
+        if (k < k1) {
+            const double2 imp = __ldg(imps + k);
+            inside = inside_impurity(position, dv2{imp.x, imp.y}, imp_r);
+        }
+        const unsigned hit = __ballot_sync(mask, inside);
+        if (hit) {
+            const int first = __popc(mask & ((1u << (__ffs(hit) - 1)) - 1u));
+            return StartScan{base - k0 + first + 1, true};
+        }
+    }
+    return StartScan{k1 - k0, false};
+}
+
 // Per-orbit counters; summed per warp before any global atomic.
 struct OrbitCounters {
     int cells;
@@ -287,9 +324,13 @@ enum TraceFlag : int { kTraceOk = 0, kTraceInside = 1, kTraceEscaped = 2, kTrace
 // identical.
 constexpr int kDeferStride = 256;
 
+//
+// start: the start-cell scan when the caller's lanes shared it
+// (start_scan_shared64), else tests < 0 and the scan runs here.
 template <int kDefer = 0>
 __device__ __forceinline__ double trace_orbit(const OrbitD& o, dv2 position, double phi, double w, const GridD& g,
-                                              int walk_cap, OrbitCounters& cnt, int& flags, int* defer = nullptr)
+                                              int walk_cap, OrbitCounters& cnt, int& flags, int* defer = nullptr,
+                                              StartScan start = StartScan{-1, false})
 {
     double lifetime = kINF;
     Isect next;
@@ -298,7 +339,13 @@ __device__ __forceinline__ double trace_orbit(const OrbitD& o, dv2 position, dou
     next.dphi = kPI2;
     next.incident_angle = phi;
 
-    {
+    if (start.tests >= 0) {
+        cnt.start_tests += start.tests;
+        if (start.inside) {
+            flags = kTraceInside;
+            return 0.0;
+        }
+    } else {
         const int pci = next.cell.y * g.cpr + next.cell.x;
         const int start = (pci == 0) ? 0 : __ldg(g.cell_end + pci - 1);
         const int end = __ldg(g.cell_end + pci);

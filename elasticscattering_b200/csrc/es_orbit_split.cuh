@@ -263,14 +263,6 @@ struct SplitCounters {
     int cells, imps, crossings, start_tests;
 };
 
-// The start-cell InsideImpurity scan (lifetime.h:90-99): the disks tested (up
-// to and including the first that holds the start) and whether one does.
-// tests < 0: not yet scanned.
-struct StartScan {
-    int tests;
-    bool inside;
-};
-
 // One disk of the scan: FP32 d^2 against r_i^2, decided in FP64 within a
 // relative 1e-4 band of the edge.
 template <class F>
