@@ -76,6 +76,12 @@ class BatchInstance(C.Structure):
                 ("temperatures", C.c_double * ES_BATCH_MAX_T)]
 
 
+class QueryMap(C.Structure):
+    """es_mlp_query_map: feature maps and sigma scale of a surrogate's queries."""
+    _fields_ = [("g_lo", C.c_double * 5), ("g_hi", C.c_double * 5), ("log_scale", C.c_int32 * 5),
+                ("sigma0_per_tau", C.c_double), ("w_per_b", C.c_double)]
+
+
 class BatchTuning(C.Structure):
     """es_batch_tuning: launch choices of a batch."""
     _fields_ = [("chunk_iters", C.c_int32), ("blocks_per_sm", C.c_int32), ("precision", C.c_int32),
@@ -147,6 +153,7 @@ CUDA_API = {
     "es_mlp_train": (_i32, [_vp, _i32, _i32, C.c_float, _u64, _vp]),
     "es_mlp_gradients": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp]),
     "es_mlp_predict": (_i32, [_vp, _vp, _i64, _vp, _vp, _vp]),
+    "es_mlp_query": (_i32, [_vp, C.POINTER(QueryMap), _vp, _i64, _vp, _vp, _vp]),
     "es_mlp_launch_count": (_i64, [_vp]),
     "es_mlp_stream": (_vp, [_vp]),
     "es_debug_trace": (_i32, [_vp, _d, _d, _i32, _i32, _d, _d, _d, _d, _d, _i32, _i32, C.POINTER(_d)]),

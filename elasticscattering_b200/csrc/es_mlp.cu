@@ -18,7 +18,11 @@
 //     GELU (forward), multiplies by GELU'(Z) (input gradient) or stores FP32
 //     (weight gradient, output layer);
 //   - small elementwise kernels: minibatch gather, loss gradient, bias
-//     gradient, Adam, ensemble mean and spread.
+//     gradient, Adam, ensemble mean and spread;
+//   - es_mlp_query's kernels: a whole query (features, every layer of every
+//     member, sigma, mean and spread) in one CUDA-core kernel for small batches
+//     (query_small_kernel, latency first), or the features and the combination
+//     around the batched tensor-core pass.
 // Every minibatch and reduction order is fixed: training is bit-reproducible.
 #include "es_cuda.h"
 #include "es_internal.h"
@@ -549,6 +553,188 @@ __global__ void to_bf16_kernel(const float* x, __nv_bfloat16* y, long long n)
     if (i < n) y[i] = __float2bfloat16(x[i]);
 }
 
+// ---- Whole queries on the device (es_mlp_query) ----------------------------
+//
+// A query is (B, T, density, impurity radius, tau). Its features are the
+// caller's maps, f = 2 (g(v) - g(lo)) / (g(hi) - g(lo)) - 1 with g = log or the
+// identity, evaluated in FP64 and rounded to FP32; the members' outputs t are
+// turned into sigma = exp(t) sigma_0 (1, w tau) / (1 + (w tau)^2) with
+// sigma_0 = sigma0_per_tau * tau and w = w_per_b * B, in FP64; the answer is the
+// members' mean and the spread is the largest over the two outputs of their
+// standard deviation over |mean|.
+
+struct QueryArgs {
+    es_mlp_query_map map;
+    const double* q;  // [n][kIn]
+    long long n;
+    const __nv_bfloat16* w16;
+    long long w16_stride;
+    long long w16_off[kLayers];
+    const float* p;
+    long long p_stride;
+    long long b_off[kLayers], w_off[kLayers];
+    float* t;           // member outputs [nets][n][kOut]
+    unsigned* counter;  // per row tile: member blocks done
+    double* sigma;      // [n][kOut]
+    double* spread;     // [n]
+    int nets;
+};
+
+__device__ __forceinline__ float query_feature(const es_mlp_query_map& mp, int k, double v)
+{
+    const double g = mp.log_scale[k] ? log(v) : v;
+    return (float)(2.0 * (g - mp.g_lo[k]) / (mp.g_hi[k] - mp.g_lo[k]) - 1.0);
+}
+
+__device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16(x)); }
+
+// One query row from its members' outputs t(k) = t[k * member_stride + c].
+__device__ __forceinline__ void combine_row(const es_mlp_query_map& mp, const double* qrow, const float* t,
+                                            long long member_stride, int nets, double* sigma, double* spread)
+{
+    const double B = qrow[0], tau = qrow[kIn - 1];
+    const double wt = mp.w_per_b * B * tau;
+    const double d = 1.0 + wt * wt;
+    const double s0 = mp.sigma0_per_tau * tau;
+    const double shape[kOut] = {1.0 / d, wt / d};
+    double worst = 0.0;
+    for (int c = 0; c < kOut; c++) {
+        double sum = 0.0;
+        for (int k = 0; k < nets; k++) sum += exp((double)__ldcg(t + k * member_stride + c)) * s0 * shape[c];
+        const double mu = sum / (double)nets;
+        double ss = 0.0;
+        for (int k = 0; k < nets; k++) {
+            const double v = exp((double)__ldcg(t + k * member_stride + c)) * s0 * shape[c] - mu;
+            ss += v * v;
+        }
+        sigma[c] = mu;
+        worst = fmax(worst, sqrt(ss / (double)nets) / fmax(fabs(mu), 1e-300));
+    }
+    *spread = worst;
+}
+
+// Small batches, latency first: block (tile, member) runs R query rows through
+// every layer of one member on the CUDA cores -- thread j owns neuron j, the
+// activations stay in shared memory, rounded to BF16 between layers as on the
+// tensor-core path, and the head is head_forward_kernel's warp-per-row sum --
+// and the last member block of a tile to finish (a counter, no waiting)
+// combines the members. Only the hidden layers' FP32 summation order differs
+// from the batched path's.
+template <int R>
+__global__ void __launch_bounds__(256) query_small_kernel(QueryArgs a)
+{
+    __shared__ float s_act[2][R][kHidden];
+    __shared__ float s_z[R][kHidden];
+    __shared__ int s_last;
+    const int tile = blockIdx.x, net = blockIdx.y, j = threadIdx.x;
+    const long long r0 = (long long)tile * R;
+    const int rows = (int)min((long long)R, a.n - r0);
+    if (j < R * kIn) {
+        const int r = j / kIn, k = j - r * kIn;
+        s_act[0][r][k] = r < rows ? bf16_round(query_feature(a.map, k, a.q[(r0 + r) * kIn + k])) : 0.0f;
+    }
+    __syncthreads();
+    const __nv_bfloat16* W16 = a.w16 + net * a.w16_stride;
+    const float* P = a.p + net * a.p_stride;
+    {  // 5 -> 256
+        float acc[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) acc[r] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < kIn; k++) {
+            const float w = __bfloat162float(W16[a.w16_off[0] + j * kIn + k]);
+#pragma unroll
+            for (int r = 0; r < R; r++) acc[r] = fmaf(w, s_act[0][r][k], acc[r]);
+        }
+        const float b = P[a.b_off[0] + j];
+#pragma unroll
+        for (int r = 0; r < R; r++) s_act[1][r][j] = bf16_round(gelu(acc[r] + b));
+    }
+    __syncthreads();
+    int cur = 1;
+    for (int l = 1; l < kLayers - 1; l++) {  // 256 -> 256
+        const uint4* wrow = reinterpret_cast<const uint4*>(W16 + a.w16_off[l] + (long long)j * kHidden);
+        float acc[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) acc[r] = 0.0f;
+        for (int k8 = 0; k8 < kHidden / 8; k8++) {
+            const uint4 wv = __ldg(wrow + k8);
+            const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const float2 w = __bfloat1622float2(w2[u]);
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    acc[r] = fmaf(w.x, s_act[cur][r][k8 * 8 + 2 * u], acc[r]);
+                    acc[r] = fmaf(w.y, s_act[cur][r][k8 * 8 + 2 * u + 1], acc[r]);
+                }
+            }
+        }
+        const float b = P[a.b_off[l] + j];
+        if (l < kLayers - 2) {
+#pragma unroll
+            for (int r = 0; r < R; r++) s_act[cur ^ 1][r][j] = bf16_round(gelu(acc[r] + b));
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) s_z[r][j] = acc[r] + b;
+        }
+        cur ^= 1;
+        __syncthreads();
+    }
+    {  // 256 -> 2 in FP32, one warp per row
+        const int warp = j >> 5, lane = j & 31;
+        const float* W = P + a.w_off[kLayers - 1];
+        const float* Bh = P + a.b_off[kLayers - 1];
+        for (int r = warp; r < rows; r += 256 / 32) {
+            float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+            for (int i = 0; i < kHidden / 32; i++) {
+                const int k = lane + 32 * i;
+                const float x = gelu(s_z[r][k]);
+                s0 += W[k] * x;
+                s1 += W[kHidden + k] * x;
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+                s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+            }
+            if (lane == 0) {
+                float* o = a.t + ((long long)net * a.n + r0 + r) * kOut;
+                o[0] = s0 + Bh[0];
+                o[1] = s1 + Bh[1];
+            }
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (j == 0) s_last = atomicAdd(a.counter + tile, 1u) == (unsigned)(a.nets - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (j < rows)
+        combine_row(a.map, a.q + (r0 + j) * kIn, a.t + (r0 + j) * kOut, a.n * kOut, a.nets, a.sigma + (r0 + j) * kOut,
+                    a.spread + r0 + j);
+}
+
+// Large batches: the features into the shared BF16 input of the batched forward pass.
+__global__ void query_features_kernel(es_mlp_query_map mp, const double* q, long long n, __nv_bfloat16* x)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * kIn) return;
+    x[i] = __float2bfloat16(query_feature(mp, (int)(i % kIn), q[i]));
+}
+
+// Large batches: members' outputs (the head's, [nets][cap][kOut]) to sigma and spread.
+__global__ void query_combine_kernel(QueryArgs a, const float* out, long long cap)
+{
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.n) return;
+    for (int k = 0; k < a.nets; k++)
+        for (int c = 0; c < kOut; c++) a.t[((long long)k * a.n + r) * kOut + c] = out[((long long)k * cap + r) * kOut + c];
+    combine_row(a.map, a.q + r * kIn, out + r * kOut, cap * kOut, a.nets, a.sigma + r * kOut, a.spread + r);
+}
+
 }  // namespace
 }  // namespace es
 
@@ -615,6 +801,14 @@ struct es_mlp {
     float* h_loss = nullptr;                 // pinned
     float* d_mean = nullptr;
     float* d_spread = nullptr;
+    // es_mlp_query staging for `qcap` queries: device and pinned host
+    long long qcap = 0;
+    double* d_q = nullptr;
+    float* d_qt = nullptr;       // member outputs [nets][qcap][kOut]
+    double* d_qout = nullptr;    // sigma [qcap][kOut], then spread [qcap]
+    unsigned* d_qcount = nullptr;  // per row tile of the small-batch kernel
+    double* h_q = nullptr;
+    double* h_qout = nullptr;
 };
 
 namespace {
@@ -671,6 +865,41 @@ es_status ensure_rows(es_mlp* m, long long rows)
     ES_MCUDA(cudaMalloc(&m->d_mean, sizeof(float) * rows * es::kOut), "ensemble mean");
     ES_MCUDA(cudaMalloc(&m->d_spread, sizeof(float) * rows * es::kOut), "ensemble spread");
     m->cap = (int)rows;
+    return ES_OK;
+}
+
+void free_query(es_mlp* m)
+{
+    cudaFree(m->d_q);
+    cudaFree(m->d_qt);
+    cudaFree(m->d_qout);
+    cudaFree(m->d_qcount);
+    if (m->h_q) cudaFreeHost(m->h_q);
+    if (m->h_qout) cudaFreeHost(m->h_qout);
+    m->d_q = m->h_q = m->d_qout = m->h_qout = nullptr;
+    m->d_qt = nullptr;
+    m->d_qcount = nullptr;
+    m->qcap = 0;
+}
+
+constexpr long long kSmallQuery = 256;  // es_mlp_query's CUDA-core kernel up to here
+constexpr int kQueryRows = 8;           // query rows per block of that kernel
+
+es_status ensure_query(es_mlp* m, long long n)
+{
+    if (n <= m->qcap) return ES_OK;
+    if (n > 4000000) return mfail(m, ES_ERR_BAD_ARG, "at most 4,000,000 queries per call");
+    free_query(m);
+    long long cap = 256;
+    while (cap < n) cap *= 2;
+    const long long tiles = (kSmallQuery + kQueryRows - 1) / kQueryRows;
+    ES_MCUDA(cudaMalloc(&m->d_q, sizeof(double) * cap * es::kIn), "query staging");
+    ES_MCUDA(cudaMalloc(&m->d_qt, sizeof(float) * m->nets * cap * es::kOut), "member outputs");
+    ES_MCUDA(cudaMalloc(&m->d_qout, sizeof(double) * cap * (es::kOut + 1)), "query answers");
+    ES_MCUDA(cudaMalloc(&m->d_qcount, sizeof(unsigned) * tiles), "query counters");
+    ES_MCUDA(cudaMallocHost(&m->h_q, sizeof(double) * cap * es::kIn), "query staging (host)");
+    ES_MCUDA(cudaMallocHost(&m->h_qout, sizeof(double) * cap * (es::kOut + 1)), "query answers (host)");
+    m->qcap = cap;
     return ES_OK;
 }
 
@@ -881,6 +1110,7 @@ es_status es_mlp_destroy(es_mlp* m)
     cudaSetDevice(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
     free_work(m);
+    free_query(m);
     cudaFree(m->d_p);
     cudaFree(m->d_g);
     cudaFree(m->d_m1);
@@ -1071,6 +1301,83 @@ es_status es_mlp_predict(es_mlp* m, const float* x, int64_t q, float* out_each, 
     if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
     ES_MCUDA(e, "surrogate query");
     return check_tc(m);
+}
+
+es_status es_mlp_query(es_mlp* m, const es_mlp_query_map* map, const double* q, int64_t n, double* out_sigma,
+                       double* out_spread, float* out_each)
+{
+    es_status st = bind_mlp(m);
+    if (st != ES_OK) return st;
+    if (!map || !q || n < 1) return mfail(m, ES_ERR_BAD_ARG, "es_mlp_query: null or empty argument");
+    for (int k = 0; k < es::kIn; k++)
+        if (!(map->g_hi[k] != map->g_lo[k]) || !std::isfinite(map->g_hi[k]) || !std::isfinite(map->g_lo[k]))
+            return mfail(m, ES_ERR_BAD_ARG, "es_mlp_query: feature map needs finite g_lo != g_hi");
+    for (int64_t i = 0; i < n; i++)
+        for (int k = 0; k < es::kIn; k++) {
+            const double v = q[i * es::kIn + k];
+            if (!std::isfinite(v) || (map->log_scale[k] && !(v > 0.0)))
+                return mfail(m, ES_ERR_BAD_ARG, "es_mlp_query: a query value is not finite (or not > 0 on a log feature)");
+        }
+    if ((st = ensure_query(m, n)) != ES_OK) return st;
+    const Layout& L = layout();
+    es::QueryArgs a{};
+    a.map = *map;
+    a.q = m->d_q;
+    a.n = n;
+    a.w16 = m->d_w16;
+    a.w16_stride = L.n_weights;
+    a.p = m->d_p;
+    a.p_stride = L.n_params;
+    for (int l = 0; l < es::kLayers; l++) {
+        a.w16_off[l] = L.w16_off[l];
+        a.b_off[l] = L.b_off[l];
+        a.w_off[l] = L.w_off[l];
+    }
+    a.t = m->d_qt;
+    a.counter = m->d_qcount;
+    a.sigma = m->d_qout;
+    a.spread = m->d_qout + n * es::kOut;
+    a.nets = m->nets;
+    std::memcpy(m->h_q, q, sizeof(double) * n * es::kIn);
+    cudaError_t e = cudaMemcpyAsync(m->d_q, m->h_q, sizeof(double) * n * es::kIn, cudaMemcpyHostToDevice, m->stream);
+    if (n <= kSmallQuery) {
+        const unsigned tiles = (unsigned)((n + kQueryRows - 1) / kQueryRows);
+        if (e == cudaSuccess) e = cudaMemsetAsync(m->d_qcount, 0, sizeof(unsigned) * tiles, m->stream);
+        if (e == cudaSuccess) {
+            if (n == 1) es::query_small_kernel<1><<<dim3(1, m->nets), 256, 0, m->stream>>>(a);
+            else es::query_small_kernel<kQueryRows><<<dim3(tiles, m->nets), 256, 0, m->stream>>>(a);
+            m->launches++;
+            e = cudaGetLastError();
+        }
+    } else {
+        if ((st = ensure_rows(m, n)) != ES_OK) return st;
+        if (e == cudaSuccess) {
+            es::query_features_kernel<<<(unsigned)((n * es::kIn + 255) / 256), 256, 0, m->stream>>>(
+                a.map, m->d_q, n, m->d_act[0]);
+            m->launches++;
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = forward(m, (int)n, true, false);
+        if (e == cudaSuccess) {
+            es::query_combine_kernel<<<(unsigned)((n + 255) / 256), 256, 0, m->stream>>>(
+                a, m->d_z[es::kLayers - 1], m->cap);
+            m->launches++;
+            e = cudaGetLastError();
+        }
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m->h_qout, m->d_qout, sizeof(double) * n * (es::kOut + 1), cudaMemcpyDeviceToHost,
+                            m->stream);
+    if (e == cudaSuccess && out_each)
+        e = cudaMemcpyAsync(out_each, m->d_qt, sizeof(float) * m->nets * n * es::kOut, cudaMemcpyDeviceToHost,
+                            m->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_tc_err, m->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, m->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    ES_MCUDA(e, "surrogate query");
+    if ((st = check_tc(m)) != ES_OK) return st;
+    if (out_sigma) std::memcpy(out_sigma, m->h_qout, sizeof(double) * n * es::kOut);
+    if (out_spread) std::memcpy(out_spread, m->h_qout + n * es::kOut, sizeof(double) * n);
+    return ES_OK;
 }
 
 int64_t es_mlp_launch_count(const es_mlp* m) { return m ? m->launches : 0; }

@@ -88,6 +88,21 @@ def untarget(q: np.ndarray, t: np.ndarray) -> np.ndarray:
     return np.exp(np.asarray(t, dtype=np.float64)) * sigma0(q[:, 4])[:, None] * drude(q)
 
 
+def query_map() -> N.QueryMap:
+    """features() and untarget() as es_mlp_query evaluates them on the device:
+    the same feature maps (log B, T, log density, r_i, log tau onto [-1, 1]) and
+    sigma = exp(t) sigma_0 Drude."""
+    m = N.QueryMap()
+    lo = (math.log(B_RANGE[0]), T_RANGE[0], math.log(N_RANGE[0]), 0.0, math.log(TAU_RANGE[0]))
+    hi = (math.log(B_RANGE[1]), T_RANGE[1], math.log(N_RANGE[1]), 2.0 * R_SCALE, math.log(TAU_RANGE[1]))
+    for k in range(5):
+        m.g_lo[k], m.g_hi[k] = lo[k], hi[k]
+        m.log_scale[k] = 1 if k in (0, 2, 4) else 0
+    m.sigma0_per_tau = float(sigma0(1.0))
+    m.w_per_b = E_CHARGE / M_EFF
+    return m
+
+
 def init_params(n_nets: int, seed: int) -> np.ndarray:
     """He-uniform weights for GELU layers, zero biases; one block per member."""
     from math import sqrt
@@ -173,6 +188,20 @@ class MLPEnsemble:
         self._check(N.cuda_lib().es_mlp_predict(self._m, x.ctypes.data, q, each.ctypes.data, mean.ctypes.data,
                                                 spread.ctypes.data))
         return each, mean, spread
+
+    def query(self, q: np.ndarray, qmap: N.QueryMap, each: bool = False):
+        """Raw queries q [n][5] -> (sigma [n][2] members' mean, spread [n], and
+        the members' outputs [n_nets][n][2] when each=True), all on the device
+        (es_mlp_query)."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        n = len(q)
+        sig = np.empty((n, 2))
+        spread = np.empty(n)
+        out_each = np.empty((self.n_nets, n, 2), dtype=np.float32) if each else None
+        self._check(N.cuda_lib().es_mlp_query(self._m, C.byref(qmap), q.ctypes.data, n, sig.ctypes.data,
+                                              spread.ctypes.data,
+                                              out_each.ctypes.data if each else None))
+        return (sig, spread, out_each) if each else (sig, spread)
 
     def launch_count(self) -> int:
         return int(N.cuda_lib().es_mlp_launch_count(self._m))
@@ -336,6 +365,7 @@ class Surrogate:
         self.ens = ensemble
         self.sim = simulator
         self.tolerance = tolerance
+        self.qmap = query_map()
 
     def fit(self, q: np.ndarray, sigma: np.ndarray, steps: int = 4000, batch: int = 256, lr: float = 1e-3,
             seed: int = 0, lr_decay_rounds: int = 4) -> list:
@@ -371,12 +401,8 @@ class Surrogate:
         """-> (sigma [n][2], fell_back [n] bool, spread [n], timings dict)."""
         q = np.asarray(q, dtype=np.float64)
         t0 = time.perf_counter()
-        each, _, _ = self.ens.predict(features(q))
-        members = untarget(q, each)                     # [n_nets][n][2] sigma
-        sig = members.mean(axis=0)
-        spread = members.std(axis=0) / np.maximum(np.abs(sig), 1e-300)
+        sig, worst = self.ens.query(q, self.qmap)       # features, members, mean and spread on the device
         t_nn = time.perf_counter() - t0
-        worst = spread.max(axis=1)
         fb = worst > self.tolerance
         t_fb = 0.0
         if fb.any():

@@ -425,6 +425,23 @@ es_status es_mlp_gradients(es_mlp* m, const float* x, const float* y, int32_t ro
  * [q][2], out_spread [q][2] (ensemble standard deviation / |mean|); any output
  * pointer may be NULL. */
 es_status es_mlp_predict(es_mlp* m, const float* x, int64_t q, float* out_each, float* out_mean, float* out_spread);
+/* Whole queries on the device: q [n][5] = (B, T, density, impurity radius,
+ * tau) -> the members' mean sigma out_sigma [n][2] and out_spread [n], the
+ * largest over the two outputs of the members' standard deviation over |mean|;
+ * out_each [n_nets][n][2] (may be NULL) receives the network outputs. The
+ * features, the five layers of every member and the conversion of the outputs
+ * to sigma (exp(t) sigma_0 (1, w tau) / (1 + (w tau)^2), FP64) run in one
+ * kernel for n <= 256 (latency: CUDA cores, activations in shared memory) and
+ * as the batched tensor-core pass plus two small kernels above. The two agree
+ * to FP32 summation order in the hidden layers. Any output may be NULL. */
+typedef struct es_mlp_query_map {
+    double g_lo[5], g_hi[5]; /* feature k: 2 (g(v) - g_lo[k]) / (g_hi[k] - g_lo[k]) - 1 */
+    int32_t log_scale[5];    /* g = log when nonzero (the query value must then be > 0), else the identity */
+    double sigma0_per_tau;   /* sigma_0 = sigma0_per_tau * tau */
+    double w_per_b;          /* omega = w_per_b * B */
+} es_mlp_query_map;
+es_status es_mlp_query(es_mlp* m, const es_mlp_query_map* map, const double* q, int64_t n, double* out_sigma,
+                       double* out_spread, float* out_each);
 int64_t es_mlp_launch_count(const es_mlp* m);
 void* es_mlp_stream(es_mlp* m);
 

@@ -82,6 +82,39 @@ def test_gradients_match_fp64_checker(cuda_device):
                 o += size
 
 
+@pytest.mark.parametrize("n", [1, 7, 256, 257, 1000])
+def test_device_query_matches_host_path(cuda_device, n):
+    """es_mlp_query (features, every member, exp/sigma_0/Drude, mean and spread
+    on the device) against the host path it replaces (features() ->
+    es_mlp_predict -> untarget() -> numpy mean and spread) and the FP64
+    checker. n <= 256 runs the one-kernel CUDA-core path, whose hidden layers
+    sum in another FP32 order than the tensor cores: its member outputs are
+    held to the checker's forward bar; n > 256 runs the batched tensor-core
+    pass on device-made features and must equal the host path to rounding."""
+    p = randomized_params(21)
+    q = S.sample_queries(n, seed=5)
+    with S.MLPEnsemble(4, cuda_device) as ens:
+        ens.set_params(p)
+        sig, spread, each = ens.query(q, S.query_map(), each=True)
+        x = S.features(q)
+        h_each, _, _ = ens.predict(x)
+    members = S.untarget(q, h_each)
+    h_sig = members.mean(axis=0)
+    h_spread = (members.std(axis=0) / np.maximum(np.abs(h_sig), 1e-300)).max(axis=1)
+    for k in range(4):
+        ref, _ = mlp_ref.forward(member(p, k), x)
+        err = np.linalg.norm(each[k] - ref) / np.linalg.norm(ref)
+        assert err <= FWD_RTOL, (k, err)
+    if n > 256:
+        assert np.allclose(each, h_each, rtol=1e-5, atol=1e-5)
+        assert np.allclose(sig, h_sig, rtol=1e-5, atol=0)
+        assert np.allclose(spread, h_spread, rtol=1e-4, atol=1e-6)
+    # either path: sigma is exp(t) sigma_0 Drude of its own member outputs, in FP64
+    own = S.untarget(q, each)
+    assert np.allclose(sig, own.mean(axis=0), rtol=1e-12, atol=0)
+    assert np.allclose(spread, (own.std(axis=0) / np.abs(own.mean(axis=0))).max(axis=1), rtol=1e-9, atol=1e-15)
+
+
 def test_training_fits_and_is_reproducible(cuda_device):
     rng = np.random.default_rng(4)
     x = rng.uniform(-1, 1, size=(4000, 5)).astype(np.float32)

@@ -80,3 +80,21 @@ def test_training_draw_stays_in_the_config4_ranges():
     in_hard = ((hard[:, 0] <= S.HARD_B[1]) | (hard[:, 4] >= S.HARD_TAU[0]) | (hard[:, 1] <= S.HARD_T[1]))
     assert in_hard.all()
     assert np.array_equal(S.training_queries(100, seed=3, hard_fraction=0.0), S.sample_queries(100, seed=3))
+
+
+def test_query_map_reproduces_features_and_untarget():
+    """The map es_mlp_query evaluates on the device, applied here in numpy with
+    the device's formula, gives features() bit for bit and untarget() to
+    rounding."""
+    m = S.query_map()
+    q = S.sample_queries(2000, seed=3)
+    f = np.empty((len(q), 5))
+    for k in range(5):
+        g = np.log(q[:, k]) if m.log_scale[k] else q[:, k]
+        f[:, k] = 2.0 * (g - m.g_lo[k]) / (m.g_hi[k] - m.g_lo[k]) - 1.0
+    assert np.array_equal(f.astype(np.float32), S.features(q))
+    t = np.random.default_rng(4).normal(size=(3, len(q), 2)).astype(np.float32)
+    wt = m.w_per_b * q[:, 0] * q[:, 4]
+    shape = np.stack([1.0 / (1.0 + wt * wt), wt / (1.0 + wt * wt)], axis=1)
+    dev = np.exp(t.astype(np.float64)) * (m.sigma0_per_tau * q[:, 4])[:, None] * shape
+    assert np.allclose(dev, S.untarget(q, t), rtol=1e-14, atol=0)
