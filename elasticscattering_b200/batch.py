@@ -94,7 +94,10 @@ class BatchSweep:
             self._b = C.c_void_p()
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library handles may already be gone
+            pass
 
     def __enter__(self):
         return self

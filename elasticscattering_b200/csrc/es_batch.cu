@@ -526,6 +526,11 @@ void drop_graph(es_batch* b)
     b->graph_dirty = true;
 }
 
+// The recorded graph no longer matches the batch's buffers or instances: it
+// is recorded again before the next launch. The executable graph is kept (and
+// never launched meanwhile) so that the new recording can update it in place.
+void invalidate_graph(es_batch* b) { b->graph_dirty = true; }
+
 void free_tables(es_batch* b)
 {
     cudaFree(b->d_table);
@@ -571,7 +576,7 @@ void free_grids(es_batch* b)
 es_status ensure_capacity(es_batch* b, int64_t n)
 {
     if (n <= b->cap) return ES_OK;
-    drop_graph(b);
+    invalidate_graph(b);
     free_tables(b);
     int64_t cap = 64;
     while (cap < n) cap *= 2;
@@ -594,7 +599,7 @@ es_status ensure_capacity(es_batch* b, int64_t n)
 es_status ensure_retrace(es_batch* b, long long want)
 {
     if (want <= b->retrace_cap) return ES_OK;
-    drop_graph(b);
+    invalidate_graph(b);
     cudaFree(b->d_retrace);
     b->d_retrace = nullptr;
     b->retrace_cap = 0;
@@ -614,7 +619,7 @@ es_status ensure_pass_scratch(es_batch* b)
         max_phase = std::max(max_phase, (long long)hi[pos].L.n_phase);
     }
     if (max_orbits <= b->lt_cap && max_phase <= b->otab_cap && b->d_partial) return ES_OK;
-    drop_graph(b);
+    invalidate_graph(b);
     free_pass_scratch(b);
     ES_BCUDA(es::dev_malloc(&b->d_lt, sizeof(double) * (size_t)max_orbits), "pass lifetimes");
     ES_BCUDA(es::dev_malloc(&b->d_otab, sizeof(double4) * (size_t)max_phase), "pass orbit table");
@@ -682,7 +687,9 @@ cudaError_t record_pass_kernels(es_batch* b)
 es_status capture(es_batch* b)
 {
     es::Range nvtx_range("batch_record");
-    drop_graph(b);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_dirty = true;
     es_status st = ES_OK;
     if (b->tuning.mode == ES_BATCH_PASS_KERNELS && (st = ensure_pass_scratch(b)) != ES_OK) return st;
     const int64_t cap = b->cap;
@@ -729,6 +736,19 @@ es_status capture(es_batch* b)
     }
     if (e_end != cudaSuccess) return bcuda(b, e_end, "batch graph capture");
     b->graph = g;
+    if (b->exec) {
+        // Same node sequence as the last recording (same passes, mode and
+        // precision): update the executable graph's parameters in place, which
+        // costs far less than instantiating it again.
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(b->exec, b->graph, &info) == cudaSuccess) {
+            b->graph_dirty = false;
+            return ES_OK;
+        }
+        cudaGetLastError();  // the failed update is not an error of a later call
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
     ES_BCUDA(cudaGraphInstantiate(&b->exec, b->graph, 0), "batch graph instantiation");
     b->graph_dirty = false;
     return ES_OK;

@@ -250,7 +250,10 @@ class SimulationCUDA:
             self._ctx = C.c_void_p()
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library handles may already be gone
+            pass
 
     def __enter__(self):
         return self
