@@ -4,9 +4,10 @@
 // No reference counterpart. Architecture 5 -> 256 x 4 -> 2, GELU, one network per
 // ensemble member. The four hidden layers (99.7% of the weights) run on the tensor
 // cores with BF16 weights and activations and FP32 accumulation: the forward pass
-// of the three 256 x 256 layers with tcgen05.mma (TMEM accumulators,
-// tc_hidden_kernel), the 5 -> 256 layer and the backward GEMMs with mma.sync
-// m16n8k16 (gemm_kernel); the 256 -> 2 output head runs in FP32 on the FP32 master
+// of the three 256 x 256 layers and their input and weight gradients with
+// tcgen05.mma (TMEM accumulators, tc_gemm_kernel), the 5 -> 256 layer's forward
+// pass and weight gradient with mma.sync m16n8k16 (gemm_kernel, its K = 5 and
+// N = 5 are below the tensor-core tile); the 256 -> 2 output head runs in FP32 on the FP32 master
 // weights and FP32 activations, because its 256 terms cancel into a small
 // output and BF16 rounding there measurably limited the fit (about 1% error in
 // sigma). FP32 master weights and Adam state. Training and inference are this
@@ -187,7 +188,8 @@ cudaError_t gemm(const GemmArgs& g, int nets, cudaStream_t s)
 
 // ---- Hidden layers 1-3 (K = N = 256) on the 5th-generation tensor cores ----
 //
-// tc_hidden_kernel: Z = A W^T + b and GELU(Z) for 128 rows x all 256 columns of
+// (The forward pass, as tc_gemm_kernel<false, false, kEpiHidden> below.)
+// Z = A W^T + b and GELU(Z) for 128 rows x all 256 columns of
 // one member per CTA (grid = row tiles x members, 512 threads), with tcgen05.mma:
 //   - the CTA stages its A tile (128 x 256 BF16, 64 KB) and the member's W
 //     (256 x 256, 128 KB, L2-resident: every row tile reads it) with 16-byte
@@ -237,7 +239,77 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned addr, unsigned parity)
     return ok != 0;
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) tc_hidden_kernel(GemmArgs g, int* err)
+// Stages rows [r0, r0 + R) x reduction [k0, k0 + kTcK) of a GEMM operand X(r, k)
+// into the no-swizzle K-major core-matrix layout at sdst (zero outside rows x
+// [0, kmax)). !T: X(r, k) = src[r * ld + k], 16-byte cp.async copies (kmax a
+// multiple of 8). T: X(r, k) = src[k * ld + r] -- the operand stored with the
+// reduction index outermost, as the backward pass reads W (input gradient) and
+// dZ and A (weight gradient) -- each thread loads 8 x 8 tiles with 16-byte loads
+// along r, transposes them in registers and stores eight 16-byte rows (rows a
+// multiple of 8). Returns after issuing (T: after storing); the caller waits
+// for the cp.async group and fences before the MMAs read.
+template <bool T, int R>
+__device__ __forceinline__ void tc_stage(unsigned sdst, const __nv_bfloat16* src, int ld, int r0, int rows, int k0,
+                                         int kmax, int tid)
+{
+    constexpr int kChunks = kTcK / 8;
+    if (!T) {
+        for (int q = tid; q < R * kChunks; q += kTcThreads) {
+            const int r = q / kChunks, kc = q % kChunks;
+            const bool in = r0 + r < rows && k0 + kc * 8 < kmax;
+            const __nv_bfloat16* p = src + (in ? (long long)(r0 + r) * ld + k0 + kc * 8 : 0);
+            const unsigned dst = sdst + ((r >> 3) * kChunks + kc) * 128 + (r & 7) * 16;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(dst), "l"(p), "r"(in ? 16 : 0)
+                         : "memory");
+        }
+    } else {
+        constexpr int kRb = R / 8;
+        for (int q = tid; q < kRb * kChunks; q += kTcThreads) {
+            const int rb = q % kRb, kb = q / kRb;
+            const bool rin = r0 + rb * 8 < rows;
+            unsigned short t[8][8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int k = k0 + kb * 8 + u;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (rin && k < kmax) v = __ldg(reinterpret_cast<const uint4*>(src + (long long)k * ld + r0 + rb * 8));
+                const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    t[u][2 * c] = (unsigned short)(w[c] & 0xFFFFu);
+                    t[u][2 * c + 1] = (unsigned short)(w[c] >> 16);
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < 8; v++) {  // row rb * 8 + v: its 8 reduction values kb * 8 + 0..7
+                const uint4 o = make_uint4((unsigned)t[0][v] | ((unsigned)t[1][v] << 16),
+                                           (unsigned)t[2][v] | ((unsigned)t[3][v] << 16),
+                                           (unsigned)t[4][v] | ((unsigned)t[5][v] << 16),
+                                           (unsigned)t[6][v] | ((unsigned)t[7][v] << 16));
+                const unsigned dst = sdst + (rb * kChunks + kb) * 128 + v * 16;
+                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" :: "r"(dst), "r"(o.x), "r"(o.y), "r"(o.z),
+                             "r"(o.w) : "memory");
+            }
+        }
+    }
+}
+
+// C[m][n] = sum_k A(m, k) B(n, k) for 128 rows x all 256 columns of one member
+// per CTA (grid = row tiles x members, 512 threads) with tcgen05.mma, the
+// reduction in steps of 256 accumulated in TMEM: the forward pass of the
+// 256 x 256 layers (kEpiHidden: Z = C + b and GELU(Z)), the input gradient
+// (TB, kEpiDGelu: C * GELU'(Z_prev) to BF16) and the weight gradient (TA, TB,
+// kEpiPlain: C in FP32). Per reduction step the CTA stages its A tile (128 x
+// 256 BF16, 64 KB) and B (256 x 256, 128 KB) in shared memory, one thread
+// issues the 16 MMAs of K = 16 (kind::f16, BF16 in, FP32 out, M = 128, N =
+// 256) and commits them to an mbarrier, and every thread waits (bounded) before
+// the next step restages; 16 warps then read the accumulator with tcgen05.ld
+// (each warp its lane quarter's rows, a quarter of the columns) for the
+// epilogue, and warp 0 frees the TMEM. Past a wait's limit the kernel records
+// kTcTimeout in *err, issues nothing more, waits once more (also bounded) and
+// frees the TMEM, so the caller gets an error instead of a hung device.
+template <bool TA, bool TB, int EPI>
+__global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(GemmArgs g, int* err)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ __align__(8) unsigned long long mbar;
@@ -250,6 +322,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_hidden_kernel(GemmArgs g, in
     const unsigned sA = (unsigned)__cvta_generic_to_shared(tc_smem);
     const unsigned sB = sA + kTcSmemA;
     const unsigned sbar = (unsigned)__cvta_generic_to_shared(&mbar);
+    constexpr int kChunks = kTcK / 8;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -260,52 +333,43 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_hidden_kernel(GemmArgs g, in
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(sbar));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    // Stage A (rows past M are zero-filled) and W: 16-byte cp.async copies into
-    // the core matrices, all of a thread's 96 copies in flight at once (a
-    // load-then-store loop would wait out one global-load latency per chunk).
-    constexpr int kChunks = kTcK / 8;  // 16-byte chunks per row
-    for (int q = tid; q < kTcM * kChunks; q += kTcThreads) {
-        const int r = q / kChunks, kc = q % kChunks;
-        const bool in = m0 + r < g.M;
-        const __nv_bfloat16* src = A + (long long)(in ? m0 + r : 0) * g.lda + kc * 8;
-        const unsigned dst = sA + ((r >> 3) * kChunks + kc) * 128 + (r & 7) * 16;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(dst), "l"(src), "r"(in ? 16 : 0)
-                     : "memory");
-    }
-    for (int q = tid; q < kTcN * kChunks; q += kTcThreads) {
-        const int n = q / kChunks, kc = q % kChunks;
-        const unsigned dst = sB + ((n >> 3) * kChunks + kc) * 128 + (n & 7) * 16;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(B + (long long)n * g.ldb + kc * 8)
-                     : "memory");
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy writes -> MMA reads
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const unsigned tmem = tmem_base;
-
-    if (tid == 0) {
+    bool done = true;
+    const int steps = (g.K + kTcK - 1) / kTcK;
+    for (int c = 0; c < steps && done; c++) {
+        const int k0 = c * kTcK;
+        tc_stage<TA, kTcM>(sA, A, g.lda, m0, g.M, k0, g.K, tid);
+        tc_stage<TB, kTcN>(sB, B, g.ldb, 0, g.N, k0, g.K, tid);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy writes -> MMA reads
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+            const unsigned tmem = tmem_base;
 #pragma unroll 1
-        for (int s = 0; s < kTcK / 16; s++) {
-            // K step s covers chunks 2s and 2s + 1 of every row group
-            const unsigned long long da = umma_desc(sA + 2 * s * 128, 128, kChunks * 128);
-            const unsigned long long db = umma_desc(sB + 2 * s * 128, 128, kChunks * 128);
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "setp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                :: "r"(tmem), "l"(da), "l"(db), "r"(kTcIdesc), "r"(s));
+            for (int s = 0; s < kTcK / 16; s++) {
+                // K step s covers chunks 2s and 2s + 1 of every row group
+                const unsigned long long da = umma_desc(sA + 2 * s * 128, 128, kChunks * 128);
+                const unsigned long long db = umma_desc(sB + 2 * s * 128, 128, kChunks * 128);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    :: "r"(tmem), "l"(da), "l"(db), "r"(kTcIdesc), "r"(c * 16 + s));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(sbar) : "memory");
         }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                     :: "r"(sbar) : "memory");
-    }
-    bool done = false;
-    for (unsigned it = 0; it < kTcWaitLimit && !done; it++) done = mbar_try_wait(sbar, 0);
-    if (!done) {
-        atomicOr(err, kTcTimeout);
-        for (unsigned it = 0; it < kTcWaitLimit && !done; it++) done = mbar_try_wait(sbar, 0);
+        bool ok = false;
+        for (unsigned it = 0; it < kTcWaitLimit && !ok; it++) ok = mbar_try_wait(sbar, (unsigned)(c & 1));
+        if (!ok) {
+            atomicOr(err, kTcTimeout);
+            for (unsigned it = 0; it < kTcWaitLimit && !ok; it++) ok = mbar_try_wait(sbar, (unsigned)(c & 1));
+        }
+        // the next step may restage only once every thread saw the MMAs finish
+        done = __syncthreads_and(ok ? 1 : 0) != 0;
+        if (!ok) done = false;
     }
     done = __all_sync(0xffffffffu, done);  // tcgen05.ld below is warp-collective
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -315,12 +379,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_hidden_kernel(GemmArgs g, in
         // warps of a lane quarter split the 256 columns, 64 each, read 32 at a
         // time; a thread holds 32 columns of its row and writes them with
         // 16-byte stores (Z skipped when out is null).
+        const unsigned tmem = tmem_base;
         const int quarter = warp & 3;
         const int col0 = (warp >> 2) * 64;
         const int m = m0 + quarter * 32 + lane;
         float* out = g.out ? g.out + net * g.strideOut : nullptr;
-        __nv_bfloat16* out2 = g.out2 + net * g.strideOut;
-        const float* bias = g.bias + net * g.strideBias;
+        __nv_bfloat16* out2 = g.out2 ? g.out2 + net * g.strideOut : nullptr;
+        const float* bias = EPI == kEpiHidden ? g.bias + net * g.strideBias : nullptr;
+        const float* zprev = EPI == kEpiDGelu ? g.zprev + net * g.strideOut : nullptr;
 #pragma unroll 1
         for (int c0 = col0; c0 < col0 + 64; c0 += 32) {
             unsigned v[32];
@@ -339,49 +405,96 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_hidden_kernel(GemmArgs g, in
 #pragma unroll
                 for (int j = 0; j < 32; j += 8) {
                     float z[8];
-                    unsigned h[4];
 #pragma unroll
-                    for (int u = 0; u < 8; u++) z[u] = __uint_as_float(v[j + u]) + bias[c0 + j + u];
+                    for (int u = 0; u < 8; u++) z[u] = __uint_as_float(v[j + u]);
+                    if (EPI == kEpiHidden) {
 #pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const __nv_bfloat162 pr = __floats2bfloat162_rn(gelu(z[2 * u]), gelu(z[2 * u + 1]));
-                        h[u] = *reinterpret_cast<const unsigned*>(&pr);
+                        for (int u = 0; u < 8; u++) z[u] += bias[c0 + j + u];
                     }
-                    if (out) {
+                    if (EPI == kEpiHidden && out) {
                         *reinterpret_cast<float4*>(out + o + j) = make_float4(z[0], z[1], z[2], z[3]);
                         *reinterpret_cast<float4*>(out + o + j + 4) = make_float4(z[4], z[5], z[6], z[7]);
                     }
-                    *reinterpret_cast<uint4*>(out2 + o + j) = make_uint4(h[0], h[1], h[2], h[3]);
+                    if (EPI == kEpiPlain) {  // weight gradients: member strides are even, not multiples of 4
+#pragma unroll
+                        for (int u = 0; u < 8; u += 2)
+                            *reinterpret_cast<float2*>(out + o + j + u) = make_float2(z[u], z[u + 1]);
+                    }
+                    if (EPI == kEpiHidden || EPI == kEpiDGelu) {
+                        unsigned h[4];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            float a0, a1;
+                            if (EPI == kEpiHidden) {
+                                a0 = gelu(z[2 * u]);
+                                a1 = gelu(z[2 * u + 1]);
+                            } else {
+                                a0 = z[2 * u] * gelu_grad(zprev[o + j + 2 * u]);
+                                a1 = z[2 * u + 1] * gelu_grad(zprev[o + j + 2 * u + 1]);
+                            }
+                            const __nv_bfloat162 pr = __floats2bfloat162_rn(a0, a1);
+                            h[u] = *reinterpret_cast<const unsigned*>(&pr);
+                        }
+                        *reinterpret_cast<uint4*>(out2 + o + j) = make_uint4(h[0], h[1], h[2], h[3]);
+                    }
                 }
             }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTcN));
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem_base), "r"(kTcN));
 }
 
-// Whether a hidden-layer GEMM can take the tensor-core kernel: K = N = 256,
-// forward (A and W both K-major), 16-byte aligned rows and member strides of
-// the operands and of the outputs (its 16-byte stores).
+namespace {
+bool al16(const void* p) { return ((unsigned long long)p & 15ull) == 0; }
+}  // namespace
+
+// Whether a GEMM can take the tensor-core kernel: N = 256 output columns, 16-byte
+// aligned operand rows and member strides, and the layout each use needs --
+// forward (kEpiHidden): A and B K-major, K = 256, lda = ldb = 256;
+// input gradient (TB, kEpiDGelu): K = 256, lda = 256, B = W with ldb = 256;
+// weight gradient (TA, TB, kEpiPlain): M a multiple of 8, any K (the rows),
+// lda = M, ldb = 256, the FP32 output 8-byte aligned (its 8-byte stores).
 bool tc_eligible(const GemmArgs& g)
 {
-    const auto al = [](const void* p) { return ((unsigned long long)p & 15ull) == 0; };
-    return g.K == kTcK && g.N == kTcN && g.lda == kTcK && g.ldb == kTcK && al(g.A) && al(g.B) &&
-           (g.strideA * 2) % 16 == 0 && (g.strideB * 2) % 16 == 0 && g.bias && g.out2 && al(g.out2) &&
-           (g.out == nullptr || al(g.out)) && g.strideOut % 8 == 0;
+    return g.K == kTcK && g.N == kTcN && g.lda == kTcK && g.ldb == kTcK && al16(g.A) && al16(g.B) &&
+           (g.strideA * 2) % 16 == 0 && (g.strideB * 2) % 16 == 0 && g.bias && g.out2 && al16(g.out2) &&
+           (g.out == nullptr || al16(g.out)) && g.strideOut % 8 == 0;
+}
+
+bool tc_eligible_dgelu(const GemmArgs& g)
+{
+    return g.K == kTcK && g.N == kTcN && g.lda == kTcK && g.ldb == kTcN && al16(g.A) && al16(g.B) &&
+           (g.strideA * 2) % 16 == 0 && (g.strideB * 2) % 16 == 0 && g.out2 && al16(g.out2) && g.zprev &&
+           g.strideOut % 8 == 0;
+}
+
+bool tc_eligible_wgrad(const GemmArgs& g)
+{
+    return g.N == kTcN && g.M % 8 == 0 && g.lda == g.M && g.ldb == kTcN && g.K >= 1 && al16(g.A) && al16(g.B) &&
+           (g.strideA * 2) % 16 == 0 && (g.strideB * 2) % 16 == 0 && g.out &&
+           ((unsigned long long)g.out & 7ull) == 0 && g.strideOut % 2 == 0;
+}
+
+template <bool TA, bool TB, int EPI>
+cudaError_t gemm_tc(const GemmArgs& g, int nets, int* err, cudaStream_t s)
+{
+    static bool attr_set = false;  // per process and instantiation; the attribute is per function
+    if (!attr_set) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(tc_gemm_kernel<TA, TB, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    tc_gemm_kernel<TA, TB, EPI><<<dim3((g.M + kTcM - 1) / kTcM, nets), kTcThreads, kTcSmem, s>>>(g, err);
+    return cudaGetLastError();
 }
 
 cudaError_t gemm_hidden_tc(const GemmArgs& g, int nets, int* err, cudaStream_t s)
 {
-    static bool attr_set = false;  // per process; the attribute is per function
-    if (!attr_set) {
-        const cudaError_t e = cudaFuncSetAttribute(tc_hidden_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
-    tc_hidden_kernel<<<dim3((g.M + kTcM - 1) / kTcM, nets), kTcThreads, kTcSmem, s>>>(g, err);
-    return cudaGetLastError();
+    return gemm_tc<false, false, kEpiHidden>(g, nets, err, s);
 }
 
 // splitmix64: the minibatch index stream (counter-based, reproducible).
@@ -796,7 +909,7 @@ struct es_mlp {
     float* d_dy = nullptr;                   // output gradient [nets][cap][kOut], FP32
     float* d_xin = nullptr;                  // query staging [cap][kIn], FP32
     float* d_loss = nullptr;                 // [nets]
-    int* d_tc_err = nullptr;                 // tc_hidden_kernel's bounded-wait flag
+    int* d_tc_err = nullptr;                 // tc_gemm_kernel's bounded-wait flag
     int* h_tc_err = nullptr;                 // pinned copy
     float* h_loss = nullptr;                 // pinned
     float* d_mean = nullptr;
@@ -985,8 +1098,9 @@ cudaError_t backward(es_mlp* m, int rows)
         gw.K = rows;
         gw.out = m->d_g + L.w_off[l];
         gw.strideOut = P;
-        // gemm writes out[n * K + k] with row stride = gw.N = K
-        e = es::gemm<true, true, es::kEpiPlain>(gw, m->nets, m->stream);
+        // out[n * K + k] with row stride = gw.N = K
+        if (es::tc_eligible_wgrad(gw)) e = es::gemm_tc<true, true, es::kEpiPlain>(gw, m->nets, m->d_tc_err, m->stream);
+        else e = es::gemm<true, true, es::kEpiPlain>(gw, m->nets, m->stream);
         m->launches++;
         if (e != cudaSuccess) break;
         es::bias_grad_kernel<<<dim3((N + 255) / 256, m->nets), 256, 0, m->stream>>>(m->d_dz[l], rows, m->cap, N,
@@ -1008,7 +1122,8 @@ cudaError_t backward(es_mlp* m, int rows)
         gx.out2 = m->d_dz[l - 1];
         gx.strideOut = (long long)m->cap * K;
         gx.zprev = m->d_z[l - 1];
-        e = es::gemm<false, true, es::kEpiDGelu>(gx, m->nets, m->stream);
+        if (es::tc_eligible_dgelu(gx)) e = es::gemm_tc<false, true, es::kEpiDGelu>(gx, m->nets, m->d_tc_err, m->stream);
+        else e = es::gemm<false, true, es::kEpiDGelu>(gx, m->nets, m->stream);
         m->launches++;
     }
     return e;
