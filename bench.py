@@ -746,6 +746,25 @@ def run_batched(args) -> None:
     e1.record(stream)
     out_fp64, mets64 = bs.collect()
     fp64_batch_ms = e0.elapsed_time(e1)
+    # the split walk with the FP64 integration: the FP64 batch's sigma bit for bit
+    exact = None
+    if tune.shape["mode"] == N.ES_BATCH_PASS_KERNELS:
+        bs.set_tuning(precision=N.ES_PRECISION_SPLIT_EXACT)
+        bs.run(with_metrics=False)
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bs.enqueue()
+        e1.record(stream)
+        out_exact, _ = bs.collect()
+        exact_ms = e0.elapsed_time(e1)
+        exact = {"ms_per_replay": exact_ms, "lifetimes_per_sec": bs.total_orbits / (exact_ms * 1e-3),
+                 "sigma_points_per_sec": len(wl.samples) * len(wl.fields) * len(wl.temperatures) / (exact_ms * 1e-3),
+                 "sigma_bit_identical_to_fp64_batch": bool(np.array_equal(out_exact, out_fp64)),
+                 "fp64_batch_ms": fp64_batch_ms,
+                 "note": "ES_PRECISION_SPLIT_EXACT: the split walk (lifetimes the FP64 walk's bit for bit) with the "
+                         "FP64 integration, one replay of the same passes"}
     bs.close()
     a, b = out_split[:, :nt, :], out_fp64[:, :nt, :]
     rel = np.abs(a - b) / np.abs(b)
@@ -941,6 +960,7 @@ def run_batched(args) -> None:
                           "above_1e-6": int((rel > 1e-6).sum()), "sigma_points_max_rel": float(prel.max()),
                           "metrics_equal": metrics_equal, "fp64_batch_ms": fp64_batch_ms,
                           "per_instance_max_rel": [float(x) for x in rel.reshape(n_pass, -1).max(axis=1)]},
+        "split_exact_batch": exact,
         "plain_fp64_path": {"passes": n_pass, "points": points, "seconds": plain_s, "points_per_sec": plain_pps,
                             "split_batch_points_per_sec": points / (step_ms * 1e-3),
                             "speedup_same_work": plain_s / (step_ms * 1e-3),

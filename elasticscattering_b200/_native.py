@@ -22,6 +22,7 @@ STATUS_NAMES = {
 }
 ES_PRECISION_FP64 = 0
 ES_PRECISION_SPLIT = 1
+ES_PRECISION_SPLIT_EXACT = 2
 
 
 class EsError(RuntimeError):

@@ -652,7 +652,7 @@ cudaError_t record_pass_kernels(es_batch* b)
         L.retrace_count = b->d_retrace_count;
         L.retrace_cap = b->retrace_cap;
         L.orbit_table = b->d_otab;
-        if (b->tuning.precision == ES_PRECISION_SPLIT)
+        if (es::split_walk(b->tuning.precision))
             e = es::launch_lifetimes_split(
                 L, es::host::long_walks(g.n_indexed, g.is.cells_per_row, g.is.cell_size, g.is.impurity_radius),
                 b->stream);
@@ -676,7 +676,7 @@ cudaError_t record_pass_kernels(es_batch* b)
         I.n_phase = L.n_phase;
         I.n_t = d.n_tau;
         I.n_blocks = es::kIntegrateBlocks;
-        I.fp32 = b->tuning.precision == ES_PRECISION_SPLIT ? 1 : 0;
+        I.fp32 = es::fp32_integrand(b->tuning.precision) ? 1 : 0;
         e = es::launch_integrate(I, b->stream);
     }
     return e;
@@ -717,7 +717,7 @@ es_status capture(es_batch* b)
         if (b->tuning.mode == ES_BATCH_PASS_KERNELS) e = record_pass_kernels(b);
         else e = es::launch_batch(L, b->tuning.precision, b->tuning.blocks_per_sm, b->n_sm, b->stream);
     }
-    if (e == cudaSuccess && b->tuning.precision == ES_PRECISION_SPLIT && b->tuning.mode != ES_BATCH_PASS_KERNELS)
+    if (e == cudaSuccess && es::split_walk(b->tuning.precision) && b->tuning.mode != ES_BATCH_PASS_KERNELS)
         e = es::launch_retrace(L, b->n_sm, b->stream);
     if (e == cudaSuccess && b->tuning.mode == ES_BATCH_PASS_KERNELS)
         e = es::copy_async(b->h_psigma, b->d_psigma, sizeof(double) * 2 * es::kBatchMaxTau * cap,
@@ -861,8 +861,10 @@ es_status es_batch_set_tuning(es_batch* b, const es_batch_tuning* t)
         return bfail(b, ES_ERR_BAD_ARG, "chunk_iters must be in [1, 4096] (got %d)", t->chunk_iters);
     if (t->blocks_per_sm != 3 && t->blocks_per_sm != 4)
         return bfail(b, ES_ERR_BAD_ARG, "blocks_per_sm must be 3 or 4 (got %d)", t->blocks_per_sm);
-    if (t->precision != ES_PRECISION_FP64 && t->precision != ES_PRECISION_SPLIT)
+    if (!es::precision_known(t->precision))
         return bfail(b, ES_ERR_BAD_ARG, "unknown precision %d", t->precision);
+    if (t->precision == ES_PRECISION_SPLIT_EXACT && t->mode != ES_BATCH_PASS_KERNELS)
+        return bfail(b, ES_ERR_BAD_ARG, "ES_PRECISION_SPLIT_EXACT runs in ES_BATCH_PASS_KERNELS mode only");
     if (t->mode != ES_BATCH_PERSISTENT && t->mode != ES_BATCH_PASS_KERNELS)
         return bfail(b, ES_ERR_BAD_ARG, "unknown batch mode %d", t->mode);
     auto item_orbits = [](const es_batch_tuning& x) {
@@ -1175,7 +1177,7 @@ es_status lay_instances(es_batch* b, const es_batch_instance* inst, int32_t n)
     b->total_items = items;
     // Re-traced orbits are a small fraction (observed ~0.05%); the list starts
     // at 1/1024 of the run and grows on overflow (es_batch_collect re-runs).
-    if (b->tuning.precision == ES_PRECISION_SPLIT)
+    if (es::split_walk(b->tuning.precision))
         if ((st = ensure_retrace(b, total / 1024 + 262144)) != ES_OK) return st;
     b->has_instances = true;
     // pass records are kernel parameters in this mode: record the graph again
@@ -1193,7 +1195,7 @@ es_status es_batch_enqueue(es_batch* b)
     es_status st = bind_batch(b);
     if (st != ES_OK) return st;
     if (!b->has_instances) return bfail(b, ES_ERR_BAD_ARG, "es_batch_set_instances has not been called");
-    if (b->tuning.precision == ES_PRECISION_SPLIT && b->retrace_cap == 0)
+    if (es::split_walk(b->tuning.precision) && b->retrace_cap == 0)
         if ((st = ensure_retrace(b, b->total_orbits / 1024 + 262144)) != ES_OK) return st;
     if (b->graph_dirty || !b->exec)
         if ((st = capture(b)) != ES_OK) return st;

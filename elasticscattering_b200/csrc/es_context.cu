@@ -175,7 +175,7 @@ es_status enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
         return fail(ctx, ES_ERR_BAD_ARG, "magnetic field must be positive and finite (got %g)", magnetic_field);
     const es::LifetimeLaunch L =
         make_launch(ctx, magnetic_field, ctx->settings.particle_speed, ctx->settings.is_clockwise ? 1 : 0, ctx->coherent);
-    if (ctx->desc.precision == ES_PRECISION_SPLIT) {
+    if (es::split_walk(ctx->desc.precision)) {
         const bool defer = es::host::long_walks(ctx->n_imps, ctx->is.cells_per_row, ctx->is.cell_size,
                                                 ctx->is.impurity_radius);
         ctx->lifetimes_valid = false;  // set again once every launch of the pass is made
@@ -241,7 +241,7 @@ es_status enqueue_integrate(es_ctx* ctx, const double* temperatures, int32_t n_t
         L.row0 = ctx->row0;
         L.rows = ctx->row1 - ctx->row0;
         L.n_blocks = es::kIntegrateBlocks;
-        L.fp32 = ctx->desc.precision == ES_PRECISION_SPLIT ? 1 : 0;
+        L.fp32 = es::fp32_integrand(ctx->desc.precision) ? 1 : 0;
         ES_CUDA(es::launch_integrate(L, ctx->stream), "integration kernel launch");
         ctx->launches += 2;
     }
@@ -340,7 +340,7 @@ es_status es_create(const es_sim_desc* desc, es_ctx** out)
                     desc->particles_per_quadrant);
     if (!(desc->region_size > 0.0) || !(desc->grid_cell_size > 0.0))
         return fail(nullptr, ES_ERR_BAD_ARG, "region_size and grid_cell_size must be positive");
-    if (desc->precision != ES_PRECISION_FP64 && desc->precision != ES_PRECISION_SPLIT)
+    if (!es::precision_known(desc->precision))
         return fail(nullptr, ES_ERR_BAD_ARG, "unknown precision %d", desc->precision);
     const int64_t n_phase = 4LL * desc->particles_per_quadrant;
     const int64_t n_pos = (int64_t)desc->positions_per_row * desc->positions_per_row;
@@ -373,12 +373,12 @@ es_status es_create(const es_sim_desc* desc, es_ctx** out)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_lifetimes, sizeof(double) * ctx->n_orbits);
     if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_phase_orbit, sizeof(es::PhaseOrbit) * n_phase);
-    if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT)
+    if (e == cudaSuccess && es::split_walk(desc->precision))
         e = es::dev_malloc(&ctx->d_orbit_table, sizeof(double4) * n_phase);
     if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_phase_sigma, sizeof(es::PhaseSigma) * n_phase);
     if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_metrics, sizeof(unsigned long long) * es::kMetCount);
     if (e == cudaSuccess) e = es::dev_malloc(&ctx->d_error, sizeof(int));
-    if (e == cudaSuccess && desc->precision == ES_PRECISION_SPLIT) {
+    if (e == cudaSuccess && es::split_walk(desc->precision)) {
         // Re-traced orbits are a small fraction (guard-band decisions); a quarter
         // of the pass is a generous bound, and overflow is reported, not ignored.
         ctx->retrace_cap = ctx->n_orbits / 4 + 1024;
@@ -443,7 +443,7 @@ es_status upload_arrays(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, co
         ES_CUDA(es::copy_async(ctx->d_imps, imp_xy, sizeof(double2) * n_indexed, kind, ctx->stream),
                 "impurity upload");
     ES_CUDA(es::copy_async(ctx->d_cell_end, cell_end, sizeof(int) * n_cells, kind, ctx->stream), "cell index upload");
-    if (ctx->desc.precision == ES_PRECISION_SPLIT) {
+    if (es::split_walk(ctx->desc.precision)) {
         if (n_indexed > ctx->imps32_cap) {
             cudaFree(ctx->d_imps32);
             ctx->d_imps32 = nullptr;

@@ -11,6 +11,15 @@
 
 namespace es {
 
+// Precision modes: the FP32/FP64 split walk (ES_PRECISION_SPLIT and
+// ES_PRECISION_SPLIT_EXACT) and the FP32 integrand (ES_PRECISION_SPLIT only).
+inline bool split_walk(int precision) { return precision == ES_PRECISION_SPLIT || precision == ES_PRECISION_SPLIT_EXACT; }
+inline bool fp32_integrand(int precision) { return precision == ES_PRECISION_SPLIT; }
+inline bool precision_known(int precision)
+{
+    return precision == ES_PRECISION_FP64 || precision == ES_PRECISION_SPLIT || precision == ES_PRECISION_SPLIT_EXACT;
+}
+
 // Device-side metric slots (es_metrics order).
 enum MetricSlot : int {
     kMetCells = 0,

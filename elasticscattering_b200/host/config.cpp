@@ -141,8 +141,9 @@ RunConfig ParseConfigText(const std::string& text, const std::string& file_path)
     if (has(values, "precision")) {
         const auto& p = values.at("precision");
         if (p == "split") cfg.precision = ES_PRECISION_SPLIT;
+        else if (p == "split_exact") cfg.precision = ES_PRECISION_SPLIT_EXACT;
         else if (p == "fp64") cfg.precision = ES_PRECISION_FP64;
-        else throw ConfigError("precision must be 'fp64' or 'split'");
+        else throw ConfigError("precision must be 'fp64', 'split' or 'split_exact'");
     }
     cfg.batched = has(values, "batched") && std::atoi(values.at("batched").c_str()) == 1;
     cfg.device_ordinal = has(values, "device_ordinal") ? std::atoi(values.at("device_ordinal").c_str()) : 0;

@@ -5,8 +5,10 @@
 // instead of the reference's print-and-exit; the CLI turns them into a
 // non-zero exit code.
 //
-// Keys this build adds (ignored by the reference): `precision fp64|split`
-// (default fp64: the reference's arithmetic), `batched 0|1` (1: every sample,
+// Keys this build adds (ignored by the reference): `precision
+// fp64|split|split_exact` (default fp64: the reference's arithmetic;
+// split_exact: the split walk with FP64 integration, the same sigma as fp64),
+// `batched 0|1` (1: every sample,
 // field and sector in one batched run), `device_ordinal n`, `journal <path>`
 // (the per-pass results journal that lets a stopped sweep resume; journal.h).
 #pragma once

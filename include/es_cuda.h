@@ -42,8 +42,12 @@ typedef enum es_status {
 } es_status;
 
 typedef enum es_precision {
-    ES_PRECISION_FP64 = 0,  /* plain FP64, reference semantics operation by operation */
-    ES_PRECISION_SPLIT = 1  /* FP32 orbit stepping, FP64 tangency band, phase and reductions */
+    ES_PRECISION_FP64 = 0,       /* plain FP64, reference semantics operation by operation */
+    ES_PRECISION_SPLIT = 1,      /* FP32 orbit stepping, FP64 tangency band, phase and reductions */
+    ES_PRECISION_SPLIT_EXACT = 2 /* the split walk (its lifetimes are the FP64 walk's bit for bit:
+                                    every decision FP32 cannot settle is taken in FP64) with the
+                                    FP64 integration: sigma equals ES_PRECISION_FP64's. Batches:
+                                    ES_BATCH_PASS_KERNELS only */
 } es_precision;
 
 /* Reference layout of ImpuritySettings (src/sim/es/settings.h:76-85). */

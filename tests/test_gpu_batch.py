@@ -267,3 +267,22 @@ def test_batch_pass_kernels_mode(sweep_inputs, reference, cuda_device, precision
         assert out[:, len(TEMPS):, :].max() == 0.0 and out[:, len(TEMPS):, :].min() == 0.0
     finally:
         b.close()
+
+
+def test_split_exact_batch_equals_fp64_batch(sweep_inputs, cuda_device):
+    """A batch in ES_PRECISION_SPLIT_EXACT (per-pass kernels: the split walk, FP64
+    integration) returns the FP64 batch's sigma bit for bit and its counters;
+    the persistent mode refuses the precision."""
+    ext, grids = sweep_inputs
+    outs, mets = {}, {}
+    for prec in (N.ES_PRECISION_FP64, N.ES_PRECISION_SPLIT_EXACT):
+        with BatchSweep(cuda_device, precision=prec, mode=N.ES_BATCH_PASS_KERNELS) as b:
+            ids = {k: b.add_grid(g) for k, g in grids.items()}
+            b.set_passes(make_passes(ext, grids, ids))
+            outs[prec], mets[prec] = b.run()
+    assert np.array_equal(outs[N.ES_PRECISION_FP64], outs[N.ES_PRECISION_SPLIT_EXACT])
+    for x, y in zip(mets[N.ES_PRECISION_FP64], mets[N.ES_PRECISION_SPLIT_EXACT]):
+        assert all(x[k] == y[k] for k in METRIC_KEYS)
+    with BatchSweep(cuda_device, precision=N.ES_PRECISION_SPLIT, mode=N.ES_BATCH_PASS_KERNELS) as b:
+        with pytest.raises(N.EsError):
+            b.set_tuning(precision=N.ES_PRECISION_SPLIT_EXACT, mode=N.ES_BATCH_PERSISTENT)

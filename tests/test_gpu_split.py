@@ -164,3 +164,35 @@ def test_split_images_and_fp32_integration(cuda_device):
         plain.close()
         split.close()
 
+
+def test_split_exact_sigma_equals_fp64(cuda_device):
+    """ES_PRECISION_SPLIT_EXACT: the split walk (lifetimes the FP64 walk's bit for
+    bit) with the FP64 integration gives the plain FP64 path's sigma and
+    per-position maps bit for bit, at B = 1 and 20 T, both sectors, three
+    temperatures; the counters are equal apart from the re-trace count."""
+    w = workloads.config1()
+    dim = 129
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    s = make_settings(w.tau, w.alpha, w.clockwise, w.particle_speed, w.region_size, w.region_extends, w.density,
+                      w.impurity_radius, w.target_cell_population)
+    temps = [1e-3, 10.0, 40.0]
+    keys = ("cells_passed", "impurities_tested", "particles_inside_impurity", "particles_escaped",
+            "particles_at_bound", "max_cells_passed", "max_impurities_tested")
+    with SimulationCUDA(dim, w.phi_steps, g.info(), device=cuda_device, precision=N.ES_PRECISION_FP64) as plain, \
+            SimulationCUDA(dim, w.phi_steps, g.info(), device=cuda_device,
+                           precision=N.ES_PRECISION_SPLIT_EXACT) as exact:
+        for coh in (True, False):
+            plain.InitSample(g, s, coh)
+            exact.InitSample(g, s, coh)
+            for B in (1.0, 20.0):
+                lp, mp = plain.ComputeLifetimes(B)
+                le, me = exact.ComputeLifetimes(B)
+                assert np.array_equal(lp.view(np.int64), le.view(np.int64)), (coh, B)
+                assert all(mp[k] == me[k] for k in keys), (coh, B)
+                sp, se = plain.DeriveTemperatures(temps), exact.DeriveTemperatures(temps)
+                assert [(x.xx, x.xy) for x in sp] == [(x.xx, x.xy) for x in se], (coh, B)
+                ip, ie = plain.ComputeSigmasWithImages(B, temps), exact.ComputeSigmasWithImages(B, temps)
+                for a, b in zip(ip, ie):
+                    assert np.array_equal(a.particle_lifetimes, b.particle_lifetimes)
+                    assert np.array_equal(a.xx_buffer, b.xx_buffer) and np.array_equal(a.xy_buffer, b.xy_buffer)

@@ -75,6 +75,8 @@ def test_parser_quirks(tmp_path, monkeypatch):
     assert d["magnetic_fields"] == [6.5]
     d = describe(write(tmp_path, BASE + "precision split\nbatched 1\ntarget_cell_population 9\n"))
     assert d["precision"] == N.ES_PRECISION_SPLIT and d["batched"] == 1 and d["target_cell_population"] == 9
+    d = describe(write(tmp_path, BASE + "precision split_exact\n", "exact.config"))
+    assert d["precision"] == N.ES_PRECISION_SPLIT_EXACT
 
 
 @pytest.mark.parametrize("edit,message", [
