@@ -1124,8 +1124,9 @@ def mlp_roofline(q: int, n_nets: int, ms: float) -> dict:
     achieved = flops / (ms * 1e-3) / 1e12
     return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "traffic": None,
-            "kernel": "tc_hidden_kernel (tcgen05.mma, BF16 in, FP32 accumulator in TMEM) for the 256 x 256 layers, "
-                      "gemm_kernel (mma.sync) for the 5 -> 256 layer, head_forward_kernel (FP32)",
+            "kernel": "es_mlp_query's batched path: query_features_kernel, tc_gemm_kernel (tcgen05.mma, BF16 in, "
+                      "FP32 accumulator in TMEM) for the 256 x 256 layers, gemm_kernel (mma.sync) for the 5 -> 256 "
+                      "layer, head_forward_kernel (FP32), query_combine_kernel; timed host to host",
             "work": f"{flops:.3g} flops per {q}-query batch, {n_nets} members", "peak_source": src,
             "note": "latency-bound: a 4096 x 256 x 256 layer is 0.27 GFLOP, a few microseconds at peak"}
 

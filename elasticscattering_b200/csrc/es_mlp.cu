@@ -570,25 +570,49 @@ __global__ void head_backward_dz_kernel(const float* dy, const float* z3, const 
 
 // Head backward, part 2: dW4[j][k] = sum_m dY[m][j] GELU(Z3[m][k]) and
 // db4[j] = sum_m dY[m][j], one thread per k (and per j for the bias), rows in order.
+// Head backward, weights: gw[c][k] = sum_m dY[m][c] GELU(Z3[m][k]) and gb[c] =
+// sum_m dY[m][c]. Block (k tile of 32, member): lane = k, warp w sums rows
+// w, w + 8, ...; the 8 warp partials are added in warp order. Fixed order: the
+// result does not depend on timing.
 __global__ void head_backward_w_kernel(const float* dy, const float* z3, int M, int cap, float* gw, float* gb,
                                        long long stride_p)
 {
+    __shared__ float s_part[8][32][kOut];
+    __shared__ float s_bias[8][kOut];
     const int net = blockIdx.y;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= kHidden) return;
-    float s0 = 0.0f, s1 = 0.0f;
-    for (int m = 0; m < M; m++) {
-        const long long row = (long long)net * cap + m;
-        const float a = gelu(z3[row * kHidden + k]);
-        s0 += dy[row * kOut] * a;
-        s1 += dy[row * kOut + 1] * a;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int k = blockIdx.x * 32 + lane;
+    const float* dyn = dy + (long long)net * cap * kOut;
+    const float* zn = z3 + (long long)net * cap * kHidden;
+    float s0 = 0.0f, s1 = 0.0f, b0 = 0.0f, b1 = 0.0f;
+    for (int m = warp; m < M; m += 8) {
+        const float a = gelu(zn[(long long)m * kHidden + k]);
+        const float d0 = dyn[(long long)m * kOut], d1 = dyn[(long long)m * kOut + 1];
+        s0 += d0 * a;
+        s1 += d1 * a;
+        b0 += d0;
+        b1 += d1;
     }
-    gw[net * stride_p + k] = s0;
-    gw[net * stride_p + kHidden + k] = s1;
-    if (k < kOut) {
-        float s = 0.0f;
-        for (int m = 0; m < M; m++) s += dy[((long long)net * cap + m) * kOut + k];
-        gb[net * stride_p + k] = s;
+    s_part[warp][lane][0] = s0;
+    s_part[warp][lane][1] = s1;
+    if (lane == 0) {
+        s_bias[warp][0] = b0;
+        s_bias[warp][1] = b1;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        float t0 = 0.0f, t1 = 0.0f;
+        for (int w = 0; w < 8; w++) {
+            t0 += s_part[w][lane][0];
+            t1 += s_part[w][lane][1];
+        }
+        gw[net * stride_p + k] = t0;
+        gw[net * stride_p + kHidden + k] = t1;
+        if (blockIdx.x == 0 && lane < kOut) {
+            float t = 0.0f;
+            for (int w = 0; w < 8; w++) t += s_bias[w][lane];
+            gb[net * stride_p + lane] = t;
+        }
     }
 }
 
@@ -616,15 +640,25 @@ __global__ void loss_kernel(const float* pred, const float* target, int M, int c
 }
 
 // db[n] = sum_m dZ[m][n] (BF16 values, FP32 sum in row order).
+// Bias gradient db[n] = sum_m dZ[m][n]: block (column tile of 32, member), lane
+// = n, warp w sums rows w, w + 8, ..., the 8 partials added in warp order.
 __global__ void bias_grad_kernel(const __nv_bfloat16* dz, int M, int cap, int N, float* db, long long stride_db)
 {
+    __shared__ float s_part[8][32];
     const int net = blockIdx.y;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = blockIdx.x * 32 + lane;
     const __nv_bfloat16* d = dz + (long long)net * cap * N;
     float s = 0.0f;
-    for (int m = 0; m < M; m++) s += __bfloat162float(d[(long long)m * N + n]);
-    db[net * stride_db + n] = s;
+    if (n < N)
+        for (int m = warp; m < M; m += 8) s += __bfloat162float(d[(long long)m * N + n]);
+    s_part[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && n < N) {
+        float t = 0.0f;
+        for (int w = 0; w < 8; w++) t += s_part[w][lane];
+        db[net * stride_db + n] = t;
+    }
 }
 
 // Adam on the FP32 master parameters; refreshes the BF16 weight copies.
@@ -1072,7 +1106,7 @@ cudaError_t backward(es_mlp* m, int rows)
     cudaError_t e = cudaSuccess;
     {
         const int last = es::kLayers - 1;
-        es::head_backward_w_kernel<<<dim3(1, m->nets), es::kHidden, 0, m->stream>>>(
+        es::head_backward_w_kernel<<<dim3(es::kHidden / 32, m->nets), 256, 0, m->stream>>>(
             m->d_dy, m->d_z[last - 1], rows, m->cap, m->d_g + L.w_off[last], m->d_g + L.b_off[last], P);
         m->launches++;
         e = cudaGetLastError();
@@ -1103,7 +1137,7 @@ cudaError_t backward(es_mlp* m, int rows)
         else e = es::gemm<true, true, es::kEpiPlain>(gw, m->nets, m->stream);
         m->launches++;
         if (e != cudaSuccess) break;
-        es::bias_grad_kernel<<<dim3((N + 255) / 256, m->nets), 256, 0, m->stream>>>(m->d_dz[l], rows, m->cap, N,
+        es::bias_grad_kernel<<<dim3((N + 31) / 32, m->nets), 256, 0, m->stream>>>(m->d_dz[l], rows, m->cap, N,
                                                                                      m->d_g + L.b_off[l], P);
         m->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) break;
