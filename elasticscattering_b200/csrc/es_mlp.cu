@@ -2,24 +2,20 @@
 // (log B, T, log density, impurity radius, log tau) to (sigma_xx, sigma_xy) / sigma_0.
 //
 // No reference counterpart. Architecture 5 -> 256 x 4 -> 2, GELU, one network per
-// ensemble member. The four hidden layers (99.7% of the weights) run on the tensor
-// cores with BF16 weights and activations and FP32 accumulation: the forward pass
-// of the three 256 x 256 layers and their input and weight gradients with
-// tcgen05.mma (TMEM accumulators, tc_gemm_kernel), the 5 -> 256 layer's forward
-// pass and weight gradient with mma.sync m16n8k16 (gemm_kernel, its K = 5 and
-// N = 5 are below the tensor-core tile); the 256 -> 2 output head runs in FP32 on the FP32 master
-// weights and FP32 activations, because its 256 terms cancel into a small
-// output and BF16 rounding there measurably limited the fit (about 1% error in
-// sigma). FP32 master weights and Adam state. Training and inference are this
-// file's kernels only:
-//   - gemm_kernel<TA, TB, EPI>: C[m][n] = sum_k A(m, k) B(n, k) for one ensemble
-//     member per blockIdx.z, with A and B read either row- or column-wise so the
-//     forward pass (X W^T), the input gradient (dZ W) and the weight gradient
-//     (dZ^T X) are all the same kernel; the epilogue adds the bias and applies
-//     GELU (forward), multiplies by GELU'(Z) (input gradient) or stores FP32
-//     (weight gradient, output layer);
-//   - small elementwise kernels: minibatch gather, loss gradient, bias
-//     gradient, Adam, ensemble mean and spread;
+// ensemble member. BF16 weights and activations, FP32 accumulation, FP32 master
+// weights and Adam state. Training and inference are this file's kernels only:
+//   - tc_gemm_kernel<TA, TB, EPI>: the three 256 x 256 layers on the
+//     5th-generation tensor cores (tcgen05.mma, TMEM accumulators): the forward
+//     pass (X W^T + b, GELU), the input gradient (dZ W times GELU'(Z_prev)) and
+//     the weight gradient (dZ^T A), with the operands transposed into the
+//     K-major shared-memory layout while staging;
+//   - input_forward_kernel / input_wgrad_kernel: the 5 -> 256 input layer on the
+//     CUDA cores (its K = 5 and N = 5 are below one tensor-core tile);
+//   - the 256 -> 2 output head in FP32 on the FP32 master weights and FP32
+//     activations, because its 256 terms cancel into a small output and BF16
+//     rounding there measurably limited the fit (about 1% error in sigma);
+//   - small kernels: minibatch gather, loss gradient, bias gradients, Adam,
+//     ensemble mean and spread;
 //   - es_mlp_query's kernels: a whole query (features, every layer of every
 //     member, sigma, mean and spread) in one CUDA-core kernel for small batches
 //     (query_small_kernel, latency first), or the features and the combination
@@ -42,11 +38,8 @@ namespace {
 constexpr int kIn = 5, kHidden = 256, kOut = 2, kLayers = 5;  // 4 hidden layers + output
 constexpr int kDims[kLayers + 1] = {kIn, kHidden, kHidden, kHidden, kHidden, kOut};
 
-constexpr int kBM = 64, kBN = 64, kBK = 32, kPad = 8;  // GEMM tile; 4 warps of 32 x 32
-
 enum Epilogue : int {
     kEpiHidden = 0,  // Z = acc + b (FP32 out), A = GELU(Z) (BF16 out2)
-    kEpiLinear = 1,  // acc + b (FP32 out)
     kEpiDGelu = 2,   // acc * GELU'(Zprev) (BF16 out2)
     kEpiPlain = 3    // acc (FP32 out)
 };
@@ -57,7 +50,7 @@ struct GemmArgs {
     long long strideA, strideB;  // per ensemble member (elements); 0 = shared
     int lda, ldb;
     int M, N, K;
-    const float* bias;  // kEpiHidden / kEpiLinear
+    const float* bias;  // kEpiHidden
     long long strideBias;
     float* out;  // FP32 [M][N], row stride N
     __nv_bfloat16* out2;  // BF16 [M][N], row stride N
@@ -74,116 +67,60 @@ __device__ __forceinline__ float gelu_grad(float x)
     return cdf + x * pdf;
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2])
+// ---- The 5 -> 256 input layer on the CUDA cores ----
+//
+// K = 5 (forward) and N = 5 (weight gradient) are below one tensor-core tile,
+// and the layer is 0.7 % of the network's multiply-adds: plain FP32 FMAs on the
+// BF16 operands (exact products), in a fixed order.
+
+// Z = X W0^T + b0 (FP32, written when z is not null) and GELU(Z) (BF16): one
+// thread per (row, neuron), the five products summed in k order.
+__global__ void input_forward_kernel(const __nv_bfloat16* x, long long stride_x, const __nv_bfloat16* w,
+                                     long long stride_w, const float* b, long long stride_b, int M, float* z,
+                                     __nv_bfloat16* act, long long stride_out)
 {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+    const int net = blockIdx.y;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)M * kHidden) return;
+    const int m = (int)(i / kHidden), n = (int)(i % kHidden);
+    const __nv_bfloat16* xr = x + net * stride_x + (long long)m * kIn;
+    const __nv_bfloat16* wr = w + net * stride_w + n * kIn;
+    float acc = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kIn; k++) acc = fmaf(__bfloat162float(xr[k]), __bfloat162float(wr[k]), acc);
+    const float zz = acc + b[net * stride_b + n];
+    if (z) z[net * stride_out + i] = zz;
+    act[net * stride_out + i] = __float2bfloat16(gelu(zz));
 }
 
-// C[m][n] = sum_k A(m, k) B(n, k); A(m, k) = TA ? A[k * lda + m] : A[m * lda + k],
-// B(n, k) = TB ? B[k * ldb + n] : B[n * ldb + k]. Out-of-range elements read as 0.
-template <bool TA, bool TB, int EPI>
-__global__ void __launch_bounds__(128) gemm_kernel(GemmArgs g)
+// dW0[n][k] = sum_m dZ0[m][n] A0[m][k]: block (32 neurons, member), lane = n,
+// warp w sums rows w, w + 8, ..., the 8 partials added in warp order.
+__global__ void input_wgrad_kernel(const __nv_bfloat16* dz, const __nv_bfloat16* a, int M, int cap, float* gw,
+                                   long long stride_p)
 {
-    __shared__ __align__(16) __nv_bfloat16 As[kBM][kBK + kPad];
-    __shared__ __align__(16) __nv_bfloat16 Bs[kBN][kBK + kPad];
-    const int net = blockIdx.z;
-    const __nv_bfloat16* A = g.A + net * g.strideA;
-    const __nv_bfloat16* B = g.B + net * g.strideB;
-    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int grp = lane >> 2, tig = lane & 3;
-    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
-
-    float acc[2][4][4];
+    __shared__ float s_part[8][32][kIn];
+    const int net = blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = blockIdx.x * 32 + lane;
+    const __nv_bfloat16* d = dz + (long long)net * cap * kHidden;
+    const __nv_bfloat16* ar = a + (long long)net * cap * kIn;
+    float s[kIn] = {};
+    for (int m = warp; m < M; m += 8) {
+        const float g = __bfloat162float(d[(long long)m * kHidden + n]);
 #pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) acc[i][j][c] = 0.0f;
-
-    for (int k0 = 0; k0 < g.K; k0 += kBK) {
-        // stage the tiles (64 x 32 each, 16 elements per thread)
-        for (int e = tid; e < kBM * kBK; e += 128) {
-            int r, c;
-            if (TA) { c = e / kBM; r = e % kBM; } else { r = e / kBK; c = e % kBK; }
-            const int m = m0 + r, k = k0 + c;
-            As[r][c] = (m < g.M && k < g.K) ? (TA ? A[(long long)k * g.lda + m] : A[(long long)m * g.lda + k]) : zero;
-        }
-        for (int e = tid; e < kBN * kBK; e += 128) {
-            int r, c;
-            if (TB) { c = e / kBN; r = e % kBN; } else { r = e / kBK; c = e % kBK; }
-            const int n = n0 + r, k = k0 + c;
-            Bs[r][c] = (n < g.N && k < g.K) ? (TB ? B[(long long)k * g.ldb + n] : B[(long long)n * g.ldb + k]) : zero;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < kBK; kk += 16) {
-            unsigned af[2][4], bf[4][2];
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-                const int r = wm + i * 16 + grp;
-                af[i][0] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * tig]);
-                af[i][1] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * tig]);
-                af[i][2] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * tig + 8]);
-                af[i][3] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * tig + 8]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int n = wn + j * 8 + grp;
-                bf[j][0] = *reinterpret_cast<const unsigned*>(&Bs[n][kk + 2 * tig]);
-                bf[j][1] = *reinterpret_cast<const unsigned*>(&Bs[n][kk + 2 * tig + 8]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], af[i], bf[j]);
-        }
-        __syncthreads();
+        for (int k = 0; k < kIn; k++) s[k] = fmaf(g, __bfloat162float(ar[(long long)m * kIn + k]), s[k]);
     }
-
-    // epilogue: element (row, col) of the 16 x 8 tile (i, j): c0, c1 at (grp, 2 tig + {0, 1}),
-    // c2, c3 at (grp + 8, 2 tig + {0, 1})
-    float* out = g.out ? g.out + net * g.strideOut : nullptr;
-    __nv_bfloat16* out2 = g.out2 ? g.out2 + net * g.strideOut : nullptr;
-    const float* bias = g.bias ? g.bias + net * g.strideBias : nullptr;
-    const float* zprev = g.zprev ? g.zprev + net * g.strideOut : nullptr;
 #pragma unroll
-    for (int i = 0; i < 2; i++)
+    for (int k = 0; k < kIn; k++) s_part[warp][lane][k] = s[k];
+    __syncthreads();
+    if (warp == 0) {
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const int m = m0 + wm + i * 16 + grp + (c >= 2 ? 8 : 0);
-                const int n = n0 + wn + j * 8 + 2 * tig + (c & 1);
-                if (m >= g.M || n >= g.N) continue;
-                const long long o = (long long)m * g.N + n;
-                const float v = acc[i][j][c];
-                if (EPI == kEpiHidden) {
-                    const float z = v + bias[n];
-                    out[o] = z;
-                    out2[o] = __float2bfloat16(gelu(z));
-                } else if (EPI == kEpiLinear) {
-                    out[o] = v + bias[n];
-                } else if (EPI == kEpiDGelu) {
-                    out2[o] = __float2bfloat16(v * gelu_grad(zprev[o]));
-                } else {
-                    out[o] = v;
-                }
-            }
-}
-
-template <bool TA, bool TB, int EPI>
-cudaError_t gemm(const GemmArgs& g, int nets, cudaStream_t s)
-{
-    const dim3 grid((g.N + kBN - 1) / kBN, (g.M + kBM - 1) / kBM, nets);
-    gemm_kernel<TA, TB, EPI><<<grid, 128, 0, s>>>(g);
-    return cudaGetLastError();
+        for (int k = 0; k < kIn; k++) {
+            float t = 0.0f;
+            for (int w = 0; w < 8; w++) t += s_part[w][lane][k];
+            gw[net * stride_p + n * kIn + k] = t;
+        }
+    }
 }
 
 // ---- Hidden layers 1-3 (K = N = 256) on the 5th-generation tensor cores ----
@@ -1080,10 +1017,17 @@ cudaError_t forward(es_mlp* m, int rows, bool shared_input, bool keep_z)
         g.strideOut = (long long)m->cap * N;
         g.out2 = m->d_act[l + 1];
         g.out = m->d_z[l];
-        // only the tensor-core kernel can skip Z
-        if (!keep_z && l + 2 < es::kLayers && es::tc_eligible(g)) g.out = nullptr;
-        if (es::tc_eligible(g)) e = es::gemm_hidden_tc(g, m->nets, m->d_tc_err, m->stream);
-        else e = es::gemm<false, false, es::kEpiHidden>(g, m->nets, m->stream);
+        if (!keep_z && l + 2 < es::kLayers) g.out = nullptr;  // Z only where the backward pass or the head reads it
+        if (l == 0) {
+            const long long n = (long long)rows * N;
+            es::input_forward_kernel<<<dim3((unsigned)((n + 255) / 256), m->nets), 256, 0, m->stream>>>(
+                g.A, g.strideA, g.B, g.strideB, g.bias, g.strideBias, rows, g.out, g.out2, g.strideOut);
+            e = cudaGetLastError();
+        } else if (es::tc_eligible(g)) {
+            e = es::gemm_hidden_tc(g, m->nets, m->d_tc_err, m->stream);
+        } else {
+            e = cudaErrorInvalidValue;  // every 256 x 256 layer meets the tensor-core kernel's layout
+        }
         m->launches++;
     }
     // the FP32 head
@@ -1133,8 +1077,15 @@ cudaError_t backward(es_mlp* m, int rows)
         gw.out = m->d_g + L.w_off[l];
         gw.strideOut = P;
         // out[n * K + k] with row stride = gw.N = K
-        if (es::tc_eligible_wgrad(gw)) e = es::gemm_tc<true, true, es::kEpiPlain>(gw, m->nets, m->d_tc_err, m->stream);
-        else e = es::gemm<true, true, es::kEpiPlain>(gw, m->nets, m->stream);
+        if (l == 0) {
+            es::input_wgrad_kernel<<<dim3(es::kHidden / 32, m->nets), 256, 0, m->stream>>>(
+                m->d_dz[0], m->d_act[0], rows, m->cap, m->d_g + L.w_off[0], P);
+            e = cudaGetLastError();
+        } else if (es::tc_eligible_wgrad(gw)) {
+            e = es::gemm_tc<true, true, es::kEpiPlain>(gw, m->nets, m->d_tc_err, m->stream);
+        } else {
+            e = cudaErrorInvalidValue;
+        }
         m->launches++;
         if (e != cudaSuccess) break;
         es::bias_grad_kernel<<<dim3((N + 31) / 32, m->nets), 256, 0, m->stream>>>(m->d_dz[l], rows, m->cap, N,
@@ -1157,7 +1108,7 @@ cudaError_t backward(es_mlp* m, int rows)
         gx.strideOut = (long long)m->cap * K;
         gx.zprev = m->d_z[l - 1];
         if (es::tc_eligible_dgelu(gx)) e = es::gemm_tc<false, true, es::kEpiDGelu>(gx, m->nets, m->d_tc_err, m->stream);
-        else e = es::gemm<false, true, es::kEpiDGelu>(gx, m->nets, m->stream);
+        else e = cudaErrorInvalidValue;
         m->launches++;
     }
     return e;
