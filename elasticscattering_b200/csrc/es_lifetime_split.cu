@@ -59,13 +59,49 @@ __global__ void orbit_table_kernel(LifetimeLaunch P)
 // so entries go to warps first: entry e runs in warp e mod W (W = the grid's
 // warps), lane (e / W) mod 32. A list of a few thousand orbits then spreads
 // over every SM, one walk per warp, instead of filling the first few blocks.
+// The counters are summed per warp, then per block in shared memory, and the
+// block adds them to the pass's counters with one atomic each (per-orbit
+// atomics on the same ten addresses serialised in L2).
 __global__ void __launch_bounds__(256, 4) lifetime_retrace_kernel(LifetimeLaunch P)
 {
+    __shared__ unsigned long long s_sum[8];
+    __shared__ unsigned s_max[2];
     const unsigned long long n_list = min(*P.retrace_count, (unsigned long long)P.retrace_cap);
     const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x / 32);
     const unsigned long long wid = (unsigned long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     const unsigned long long lane = threadIdx.x & 31;
-    for (unsigned long long e = lane * warps + wid; e < n_list; e += 32 * warps) retrace_orbit(P, P.retrace[e]);
+    if (threadIdx.x < 8) s_sum[threadIdx.x] = 0ull;
+    if (threadIdx.x < 2) s_max[threadIdx.x] = 0u;
+    __syncthreads();
+    OrbitCounters cnt = {0, 0, 0, 0};
+    unsigned in = 0, esc = 0, bound = 0, mc = 0, mi = 0, n = 0;
+    for (unsigned long long e = lane * warps + wid; e < n_list; e += 32 * warps) {
+        retrace_orbit(P, P.retrace[e], cnt, in, esc, bound, mc, mi);
+        n++;
+    }
+    const unsigned v[8] = {(unsigned)cnt.cells, (unsigned)cnt.imps, (unsigned)cnt.crossings,
+                           (unsigned)cnt.start_tests, in, esc, bound, n};
+    unsigned r[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) r[k] = __reduce_add_sync(0xffffffffu, v[k]);
+    const unsigned rmc = __reduce_max_sync(0xffffffffu, mc), rmi = __reduce_max_sync(0xffffffffu, mi);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (r[k]) atomicAdd(&s_sum[k], (unsigned long long)r[k]);
+        atomicMax(&s_max[0], rmc);
+        atomicMax(&s_max[1], rmi);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int slot[8] = {kMetCells, kMetImps, kMetCrossings, kMetStartTests, kMetInside, kMetEscaped, kMetAtBound,
+                             kMetRetraced};
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (s_sum[k]) atomicAdd(P.metrics + slot[k], s_sum[k]);
+        if (s_max[0]) atomicMax(P.metrics + kMetMaxCells, (unsigned long long)s_max[0]);
+        if (s_max[1]) atomicMax(P.metrics + kMetMaxImps, (unsigned long long)s_max[1]);
+    }
 }
 
 // Cell-local FP32 copy of the ordered impurities: x - (start + cx L), y - (start + cy L).

@@ -842,8 +842,11 @@ __device__ __forceinline__ bool split_orbit_synced(const F& f, long long g, unsi
 }
 
 // Exact FP64 TraceOrbit of orbit g (src/sim/es/lifetime.h:78-148): writes the
-// lifetime and adds the orbit's metrics.
-__device__ __forceinline__ void retrace_orbit(const LifetimeLaunch& P, long long g)
+// lifetime and adds the orbit's counters to `cnt` (and its flags' counts to
+// `in`, `esc`, `bound`, its maxima to `max_cells`, `max_imps`).
+__device__ __forceinline__ void retrace_orbit(const LifetimeLaunch& P, long long g, OrbitCounters& cnt,
+                                              unsigned& in, unsigned& esc, unsigned& bound, unsigned& max_cells,
+                                              unsigned& max_imps)
 {
     GridD gr;
     gr.imps = P.imps;
@@ -855,21 +858,20 @@ __device__ __forceinline__ void retrace_orbit(const LifetimeLaunch& P, long long
     gr.cpr = P.cpr;
     dv2 pos;
     const OrbitD o = make_orbit(P, g, pos);
-    OrbitCounters cnt = {0, 0, 0, 0};
+    OrbitCounters c = {0, 0, 0, 0};
     int flags = kTraceOk;
-    const double lt = trace_orbit(o, pos, o.particle_angle, P.w, gr, P.walk_cap, cnt, flags);
+    const double lt = trace_orbit(o, pos, o.particle_angle, P.w, gr, P.walk_cap, c, flags);
     if (flags & kTraceWalkCap) atomicOr(P.error, kErrWalkCap);
     P.out[g] = lt;
-    atomicAdd(P.metrics + kMetCells, (unsigned long long)cnt.cells);
-    atomicAdd(P.metrics + kMetImps, (unsigned long long)cnt.imps);
-    atomicAdd(P.metrics + kMetCrossings, (unsigned long long)cnt.crossings);
-    atomicAdd(P.metrics + kMetStartTests, (unsigned long long)cnt.start_tests);
-    if (flags & kTraceInside) atomicAdd(P.metrics + kMetInside, 1ull);
-    if (flags & kTraceEscaped) atomicAdd(P.metrics + kMetEscaped, 1ull);
-    if (flags & kTraceAtBound) atomicAdd(P.metrics + kMetAtBound, 1ull);
-    atomicMax(P.metrics + kMetMaxCells, (unsigned long long)cnt.cells);
-    atomicMax(P.metrics + kMetMaxImps, (unsigned long long)cnt.imps);
-    atomicAdd(P.metrics + kMetRetraced, 1ull);
+    cnt.cells += c.cells;
+    cnt.imps += c.imps;
+    cnt.crossings += c.crossings;
+    cnt.start_tests += c.start_tests;
+    in += (flags & kTraceInside) ? 1u : 0u;
+    esc += (flags & kTraceEscaped) ? 1u : 0u;
+    bound += (flags & kTraceAtBound) ? 1u : 0u;
+    max_cells = max(max_cells, (unsigned)c.cells);
+    max_imps = max(max_imps, (unsigned)c.imps);
 }
 
 // Metrics of the lanes in `mask` (one instance), one atomic per warp and counter.
