@@ -127,11 +127,10 @@ class BatchSweep:
         if isinstance(grid, DeviceGrid):
             self._check(N.cuda_lib().es_batch_add_dgrid(self._b, grid.handle, C.byref(out)))
             return int(out.value)
-        xy = grid.GetImpurities()
-        idx = grid.GetIndex()
+        # the host Grid's own arrays, read in place by the library
+        xy, n, idx = grid.arrays()
         s = grid.GetSettings()
-        self._check(N.cuda_lib().es_batch_add_grid(self._b, xy.ctypes.data, len(xy), idx.ctypes.data, C.byref(s),
-                                                   C.byref(out)))
+        self._check(N.cuda_lib().es_batch_add_grid(self._b, xy, n, idx, C.byref(s), C.byref(out)))
         return int(out.value)
 
     def clear(self) -> None:

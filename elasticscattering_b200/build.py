@@ -39,6 +39,7 @@ CUDA_UNITS = {
     "es_integrate.cu": ["-fmad=false"],
     "es_probe.cu": [],
     "es_fault.cu": [],
+    "es_upload.cu": [],  # pinned staging of pageable grid uploads (host threads)
     # FP32 walk: built without contraction as well. Its FP64 parts (winner
     # time, re-trace) must keep the reference's rounding, and contracting the
     # FP32 part alone was measured at 1 % faster while changing guard-band
@@ -100,7 +101,7 @@ def build_cuda(verbose_ptxas: bool = False, force: bool = False) -> Path:
     with ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
         list(ex.map(_run, jobs))
     if force or jobs or _stale(out, objs):
-        _run([nvcc()] + ARCH + ["-shared", "-o", str(out)] + [str(o) for o in objs])
+        _run([nvcc()] + ARCH + ["-shared", "-Xcompiler", "-pthread", "-o", str(out)] + [str(o) for o in objs])
     return out
 
 

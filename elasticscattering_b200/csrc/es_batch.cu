@@ -45,6 +45,7 @@
 #include "es_host_math.h"
 #include "es_orbit_split.cuh"
 #include "es_sigma32.cuh"
+#include "es_upload.h"
 
 #include <algorithm>
 #include <cmath>
@@ -427,6 +428,7 @@ struct es_batch_grid {
     int* d_cell_end = nullptr;
     int64_t n_indexed = 0;
     es_impurity_settings is{};
+    int64_t imps_cap = 0, cells_cap = 0;  // allocated impurities and cells
 };
 
 struct es_batch_phase {
@@ -447,6 +449,11 @@ struct es_batch {
     std::vector<long long> pass_items;        // work items per pass, kernel order
 
     std::vector<es_batch_grid> grids;
+    // Device memory of the grids es_batch_clear released, reused by the next
+    // es_batch_add_grid calls (smallest that fits): a sweep that clears and adds
+    // grids of the same sizes every step allocates and frees nothing.
+    std::vector<es_batch_grid> spare;
+    es::Staging staging;  // pinned ring for grids copied from pageable host memory
     std::map<std::tuple<int, int, double, double, int>, es_batch_phase> phases;  // (ppq, coherent, alpha, speed, cw)
 
     // instances (caller order) and their host-side constants
@@ -558,14 +565,20 @@ void free_pass_scratch(es_batch* b)
     b->lt_cap = b->otab_cap = 0;
 }
 
+void free_grid(es_batch_grid& g)
+{
+    cudaFree(g.d_imps);
+    cudaFree(g.d_imps32);
+    cudaFree(g.d_cell_end);
+    g = es_batch_grid{};
+}
+
 void free_grids(es_batch* b)
 {
-    for (auto& g : b->grids) {
-        cudaFree(g.d_imps);
-        cudaFree(g.d_imps32);
-        cudaFree(g.d_cell_end);
-    }
+    for (auto& g : b->grids) free_grid(g);
     b->grids.clear();
+    for (auto& g : b->spare) free_grid(g);
+    b->spare.clear();
     for (auto& kv : b->phases) {
         cudaFree(kv.second.d_orbit);
         cudaFree(kv.second.d_sigma);
@@ -840,6 +853,7 @@ es_status es_batch_destroy(es_batch* b)
     cudaFree(b->d_retrace_count);
     if (b->h_error) cudaFreeHost(b->h_error);
     if (b->h_retrace_count) cudaFreeHost(b->h_retrace_count);
+    b->staging.release();
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return ES_OK;
@@ -941,23 +955,43 @@ es_status add_grid_arrays(es_batch* b, const double* imp_xy, int64_t n_indexed, 
                           const es_impurity_settings* is, cudaMemcpyKind kind, int32_t* out_grid)
 {
     const int64_t n_cells = (int64_t)is->cells_per_row * is->cells_per_row;
+    const int64_t n_alloc = n_indexed > 0 ? n_indexed : 1;
     es_batch_grid g;
+    // the smallest cleared allocation that holds this grid; when none does, the
+    // cleared ones are released before a new one is made
+    int best = -1;
+    for (size_t k = 0; k < b->spare.size(); k++) {
+        const es_batch_grid& c = b->spare[k];
+        if (c.imps_cap >= n_alloc && c.cells_cap >= n_cells && (best < 0 || c.imps_cap < b->spare[(size_t)best].imps_cap))
+            best = (int)k;
+    }
+    cudaError_t e = cudaSuccess;
+    if (best >= 0) {
+        g = b->spare[(size_t)best];
+        b->spare.erase(b->spare.begin() + best);
+    } else {
+        for (auto& c : b->spare) free_grid(c);
+        b->spare.clear();
+        e = es::dev_malloc(&g.d_imps, sizeof(double2) * (size_t)n_alloc);
+        if (e == cudaSuccess) e = es::dev_malloc(&g.d_imps32, sizeof(float2) * (size_t)n_alloc);
+        if (e == cudaSuccess) e = es::dev_malloc(&g.d_cell_end, sizeof(int) * (size_t)n_cells);
+        g.imps_cap = n_alloc;
+        g.cells_cap = n_cells;
+    }
     g.n_indexed = n_indexed;
     g.is = *is;
-    const size_t n_alloc = (size_t)(n_indexed > 0 ? n_indexed : 1);
-    cudaError_t e = es::dev_malloc(&g.d_imps, sizeof(double2) * n_alloc);
-    if (e == cudaSuccess) e = es::dev_malloc(&g.d_imps32, sizeof(float2) * n_alloc);
-    if (e == cudaSuccess) e = es::dev_malloc(&g.d_cell_end, sizeof(int) * n_cells);
-    if (e == cudaSuccess && n_indexed > 0) e = es::copy_async(g.d_imps, imp_xy, sizeof(double2) * n_indexed, kind, b->stream);
-    if (e == cudaSuccess) e = es::copy_async(g.d_cell_end, cell_end, sizeof(int) * n_cells, kind, b->stream);
+    auto upload = [&](void* dst, const void* src, size_t bytes) {
+        return kind == cudaMemcpyHostToDevice ? b->staging.h2d(dst, src, bytes, b->stream)
+                                              : es::copy_async(dst, src, bytes, kind, b->stream);
+    };
+    if (e == cudaSuccess && n_indexed > 0) e = upload(g.d_imps, imp_xy, sizeof(double2) * (size_t)n_indexed);
+    if (e == cudaSuccess) e = upload(g.d_cell_end, cell_end, sizeof(int) * (size_t)n_cells);
     if (e == cudaSuccess)
         e = es::launch_local_impurities(g.d_imps, g.d_cell_end, g.d_imps32, is->spawn_region_start, is->cell_size,
                                         is->cells_per_row, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) {
-        cudaFree(g.d_imps);
-        cudaFree(g.d_imps32);
-        cudaFree(g.d_cell_end);
+        free_grid(g);
         return bcuda(b, e, "es_batch_add_grid");
     }
     b->launches++;
@@ -975,7 +1009,8 @@ es_status es_batch_clear(es_batch* b)
     es_status st = bind_batch(b);
     if (st != ES_OK) return st;
     ES_BCUDA(cudaStreamSynchronize(b->stream), "stream synchronize");
-    free_grids(b);
+    for (auto& g : b->grids) b->spare.push_back(g);
+    b->grids.clear();
     b->inst.clear();
     b->has_instances = false;
     return ES_OK;

@@ -10,6 +10,7 @@
 #include "es_host_math.h"
 #include "es_nvtx.h"
 #include "es_internal.h"
+#include "es_upload.h"
 
 #include <cfloat>
 #include <cmath>
@@ -43,6 +44,7 @@ struct es_ctx {
     es_impurity_settings is{};
     uint64_t generation = 0;
     bool has_grid = false;
+    es::Staging staging;  // pinned ring for grids uploaded from pageable host memory
 
     // sector (Simulation::InitSample state)
     es_settings settings{};
@@ -317,6 +319,7 @@ void release(es_ctx* ctx)
     cudaFree(ctx->d_retrace);
     cudaFree(ctx->d_retrace_count);
     if (ctx->h_sigma) cudaFreeHost(ctx->h_sigma);
+    ctx->staging.release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -439,10 +442,12 @@ es_status upload_arrays(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, co
         ES_CUDA(es::dev_malloc(&ctx->d_cell_end, sizeof(int) * n_cells), "cell index buffer");
         ctx->cells_cap = n_cells;
     }
-    if (n_indexed > 0)
-        ES_CUDA(es::copy_async(ctx->d_imps, imp_xy, sizeof(double2) * n_indexed, kind, ctx->stream),
-                "impurity upload");
-    ES_CUDA(es::copy_async(ctx->d_cell_end, cell_end, sizeof(int) * n_cells, kind, ctx->stream), "cell index upload");
+    auto upload = [&](void* dst, const void* src, size_t bytes) {
+        return kind == cudaMemcpyHostToDevice ? ctx->staging.h2d(dst, src, bytes, ctx->stream)
+                                              : es::copy_async(dst, src, bytes, kind, ctx->stream);
+    };
+    if (n_indexed > 0) ES_CUDA(upload(ctx->d_imps, imp_xy, sizeof(double2) * n_indexed), "impurity upload");
+    ES_CUDA(upload(ctx->d_cell_end, cell_end, sizeof(int) * n_cells), "cell index upload");
     if (es::split_walk(ctx->desc.precision)) {
         if (n_indexed > ctx->imps32_cap) {
             cudaFree(ctx->d_imps32);

@@ -137,6 +137,15 @@ class Grid:
         p = N.host_lib().es_grid_index(self._h)
         return np.ctypeslib.as_array(p, shape=(c * c,)).copy()
 
+    def arrays(self) -> tuple:
+        """(impurity x,y pairs, their count, cell index) as pointers into this
+        Grid's own host memory, valid while the Grid lives: what es_upload_grid
+        and es_batch_add_grid read, without a copy."""
+        n = self.GetTotalImpurityCount()
+        xy = C.cast(N.host_lib().es_grid_impurities(self._h), C.c_void_p) if n else None
+        idx = C.cast(N.host_lib().es_grid_index(self._h), C.c_void_p)
+        return xy, n, idx
+
     def info(self) -> "GridInformation":
         return GridInformation(self.region_size, self.region_extends, self.GetSettings().cell_size,
                                self.GetTotalImpurityCount(), self.GetCellsPerRow() ** 2)
@@ -272,12 +281,10 @@ class SimulationCUDA:
         if isinstance(grid, DeviceGrid):
             self._check(N.cuda_lib().es_upload_dgrid(self._ctx, grid.handle))
             return
-        xy = grid.GetImpurities()
-        idx = grid.GetIndex()
+        xy, n, idx = grid.arrays()
         s = grid.GetSettings()
         gen = int(N.host_lib().es_grid_generation(grid.handle))
-        self._check(N.cuda_lib().es_upload_grid(self._ctx, xy.ctypes.data, len(xy), idx.ctypes.data, C.byref(s),
-                                                gen))
+        self._check(N.cuda_lib().es_upload_grid(self._ctx, xy, n, idx, C.byref(s), gen))
 
     def upload_grid(self, grid: Grid) -> None:
         self._upload(grid)

@@ -144,7 +144,8 @@ es_status es_set_rows(es_ctx* ctx, int32_t j0, int32_t j1);
  * the cumulative end index of each of cells_per_row^2 cells (Grid::GetIndex,
  * src/sim/Grid.h:75). The upload is skipped when `generation` equals the
  * generation already resident (the reference keys on the seed, which is 0 for
- * every file-loaded grid). */
+ * every file-loaded grid). Pageable host arrays are copied through a pinned
+ * staging ring by several host threads; pinned arrays are copied directly. */
 es_status es_upload_grid(es_ctx* ctx, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
                          const es_impurity_settings* is, uint64_t generation);
 
@@ -335,11 +336,17 @@ es_status es_batch_get_tuning(const es_batch* b, es_batch_tuning* out);
 es_status es_batch_set_tuning(es_batch* b, const es_batch_tuning* t);
 
 /* Copies one impurity grid (same arrays as es_upload_grid) to the device and
- * returns its index in *out_grid. Grids stay resident until es_batch_clear. */
+ * returns its index in *out_grid. Grids stay resident until es_batch_clear.
+ * Host arrays in pageable memory are copied through a pinned staging ring by
+ * several host threads; pinned arrays are copied directly. */
 es_status es_batch_add_grid(es_batch* b, const double* imp_xy, int64_t n_indexed, const int32_t* cell_end,
                             const es_impurity_settings* is, int32_t* out_grid);
 
-/* Releases every grid and instance of the batch. */
+/* Releases every grid and instance of the batch. The grids' device memory is
+ * kept and reused by later es_batch_add_grid calls (the smallest allocation
+ * that fits; when none fits, all kept memory is freed before the new grid is
+ * allocated), so a sweep that clears and adds same-sized grids every step
+ * neither allocates nor frees. es_batch_destroy frees everything. */
 es_status es_batch_clear(es_batch* b);
 
 /* Sets the passes of the batch (validated as es_create / es_init_sample /
