@@ -182,7 +182,7 @@ es_status enqueue_lifetimes(es_ctx* ctx, double magnetic_field)
                                                 ctx->is.impurity_radius);
         ctx->lifetimes_valid = false;  // set again once every launch of the pass is made
         ES_CUDA(es::launch_lifetimes_split(L, defer, ctx->stream), "split lifetime kernel launch");
-        ctx->launches += 3;  // orbit table, lifetime walk, FP64 re-trace
+        ctx->launches += defer ? 4 : 3;  // orbit table, lifetime walk, (winner finish,) FP64 re-trace
     } else {
         ctx->lifetimes_valid = false;
         ES_CUDA(es::launch_lifetimes_fp64(L, ctx->stream), "lifetime kernel launch");

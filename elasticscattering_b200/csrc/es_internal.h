@@ -142,10 +142,11 @@ void dgrid_arrays(const es_dgrid* g, const double2** imps, const int** cell_end,
                   es_impurity_settings* is, uint64_t* generation, int* device);
 
 cudaError_t launch_lifetimes_fp64(const LifetimeLaunch& L, cudaStream_t s);
-// Split precision: FP32 walk, then the FP64 re-trace of the listed orbits (two
-// launches, after the orbit table's). defer_finish: take each winner's FP64
-// time after a warp sync (passes with long walks; see lifetime_split_kernel).
-cudaError_t launch_lifetimes_split(const LifetimeLaunch& L, bool defer_finish, cudaStream_t s);
+// Split precision: the orbit table, the FP32 walk, then the FP64 re-trace of
+// the listed orbits. split_finish (passes with long walks): the walk leaves
+// each winner's FP64 time to a finish kernel between walk and re-trace (see
+// lifetime_split_kernel); otherwise the walk takes it.
+cudaError_t launch_lifetimes_split(const LifetimeLaunch& L, bool split_finish, cudaStream_t s);
 cudaError_t launch_local_impurities(const double2* imps, const int* cell_end, float2* out, double start, double cell,
                                     int cpr, cudaStream_t s);
 // Stages (b)+(c) for one temperature group: two launches.

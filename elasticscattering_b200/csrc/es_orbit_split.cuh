@@ -801,44 +801,73 @@ __device__ __forceinline__ bool split_orbit(const F& f, long long g, SplitCounte
     return false;
 }
 
-// split_orbit with the winner's FP64 time taken after a warp sync. `mask`
-// names the lanes of the warp that call this for one orbit each. Lanes end
-// their walks after different numbers of cell steps; they meet at a __syncwarp
-// before the FP64 winner recompute, so that code (sqrt, asin and divisions of
-// the reference's GetCrossPoints/GetAngle) runs once per warp instead of once
-// per distinct exit step: 3% faster on B200 per single-pass launch of 257^2 x
-// 516 orbits at 5e15 m^-2. Every lane reaches the sync: the walk is bounded by
-// the walk cap and every path returns. The batched kernels keep split_orbit (the
-// deferred form measured 7% slower there, where the orbit's integrand follows
-// the walk in the same kernel).
+// Lifetime slot of an orbit whose walk found its winning disk(s) but whose
+// FP64 time is still to be taken (lifetime_finish_kernel): a negative double
+// (lifetimes are >= 0) with the first disk in the low word and the second + 1
+// (0: none) in the high word's low 31 bits.
+__device__ __forceinline__ double encode_hit(int2 win)
+{
+    return __hiloint2double((int)(0x80000000u | (unsigned)(win.y + 1)), win.x);
+}
+
+__device__ __forceinline__ bool decode_hit(double v, int2& win)
+{
+    const long long b = __double_as_longlong(v);
+    if (b >= 0) return false;
+    win.x = (int)(unsigned)(b & 0xffffffffLL);
+    win.y = (int)(((unsigned long long)b >> 32) & 0x7fffffffu) - 1;
+    return true;
+}
+
+// A re-trace list entry made by lifetime_finish_kernel (an orbit whose walk
+// was already counted): bit 62 of the orbit index.
+constexpr long long kRetraceFromFinish = 1LL << 62;
+
+// The split walk of orbit g up to its winning disk(s), for passes whose walks
+// end after differing numbers of cell steps: the FP64 time of the winner --
+// sqrt, asin and divisions of the reference's GetCrossPoints/GetAngle -- is
+// left to lifetime_finish_kernel, which runs it for every such orbit of the
+// pass with all lanes busy and none of the walk's registers live. Returns
+// kSplitDone (lt set), kSplitHit (win set) or kSplitRetrace (cnt and flags
+// cleared). `mask`: the warp's lanes that call this together (their start scan
+// is shared when they start at one position).
 template <class F>
-__device__ __forceinline__ bool split_orbit_synced(const F& f, long long g, unsigned mask, SplitCounters& cnt,
-                                                   int& flags, double& lt)
+__device__ __forceinline__ int split_orbit_walk(const F& f, long long g, unsigned mask, SplitCounters& cnt, int& flags,
+                                                double& lt, int2& win)
 {
     dv2 pos;
     const OrbitD o = make_orbit(f, g, pos);
     cnt = SplitCounters{0, 0, 0, 0};
     flags = kTraceOk;
     lt = 0.0;
-    int st = kSplitDone;
-    int2 win = make_int2(-1, -1);
+    win = make_int2(-1, -1);
     const int cx = (int)((pos.x - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
     const int cy = (int)((pos.y - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
     const bool in_grid = !(cx < 0 || cy < 0 || cx >= f.cpr() || cy >= f.cpr());
     const StartScan start = warp_start_scan(f, pos, cx, cy, in_grid, mask);
-    if (!in_grid) atomicOr(f.error(), kErrStartCell);
-    else st = trace_split<F, true>(f, o, pos, cnt, flags, lt, win, start);
-    __syncwarp(mask);
-    if (st == kSplitHit) {
-        lt = finish_hit(f, o, win.x, win.y, flags);
-        st = (lt != lt) ? kSplitRetrace : kSplitDone;  // NaN: a crossing point the reference drops
+    if (!in_grid) {
+        atomicOr(f.error(), kErrStartCell);
+        return kSplitDone;
     }
+    const int st = trace_split<F, true>(f, o, pos, cnt, flags, lt, win, start);
     if (st == kSplitRetrace) {
         cnt = SplitCounters{0, 0, 0, 0};
         flags = kTraceOk;
-        return true;
     }
-    return false;
+    return st;
+}
+
+// The counters split_orbit_walk gave orbit g (the walk is deterministic):
+// what the pass already counted for an orbit that lifetime_finish_kernel
+// hands to the FP64 re-trace.
+__device__ __forceinline__ SplitCounters split_walk_counters(const LifetimeLaunch& P, long long g)
+{
+    SplitCounters cnt;
+    int flags;
+    double lt;
+    int2 win;
+    split_orbit_walk(LaunchFields{P}, g, 0u, cnt, flags, lt, win);
+    return cnt;
 }
 
 // Exact FP64 TraceOrbit of orbit g (src/sim/es/lifetime.h:78-148): writes the
