@@ -490,7 +490,8 @@ def run_ours(args) -> None:
         achieved = k["flops"] / (k["ms"] * 1e-3) / 1e12
         return {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None, "traffic": profiled_traffic(name, w.orbits_per_pass),
-                "kernel": "lifetime_split_kernel + lifetime_retrace_kernel" if name == "split" else "lifetime_fp64_kernel",
+                "kernel": ("lifetime_split_kernel + lifetime_finish_kernel + lifetime_retrace_kernel" if name == "split"
+                           else "lifetime_fp64_kernel"),
                 "work": "algorithmic FP64-op count of the reference's TraceOrbit (flop_model) per launch",
                 "peak_source": peak_src, "flop_model": FLOP_MODEL, "per_launch": k["per_launch"],
                 "avg_launch_ms": k["ms"] / len(k["per_launch"]), "retraced_fp64": k["retraced_fp64"],
@@ -729,11 +730,10 @@ def run_batched(args) -> None:
     orbits = bs.total_orbits
     nt = len(wl.temperatures)
     points = len(wl.samples) * len(wl.fields) * nt
-    if tune.shape["mode"] == N.ES_BATCH_PASS_KERNELS:
-        # per pass: orbit table, lifetime walk, FP64 re-trace, integration, reduction
-        kernels_per_replay = 5 * n_pass
-    else:
-        kernels_per_replay = 2  # the persistent kernel and the FP64 re-trace
+    # counted from the recorded graph: per pass the orbit table, the lifetime walk,
+    # the winners' FP64 finish (long-walk passes), the FP64 re-trace, integration
+    # and reduction; or the persistent kernel and its FP64 re-trace
+    kernels_per_replay = bs.graph_kernels()
     alg_flops = sum(lifetime_flops(m, 0) for m in mets) + FLOP_MODEL["per_orbit"] * orbits
     retraced = sum(m["retraced_fp64"] for m in mets)
 
@@ -950,7 +950,8 @@ def run_batched(args) -> None:
                      "traffic": (profiled_traffic("split", orbits / n_pass)
                                  if tune.shape["mode"] == N.ES_BATCH_PASS_KERNELS
                                  else profiled_traffic("batch_kernel_config2.md")),
-                     "kernel": "lifetime_split_kernel + lifetime_retrace_kernel (per pass, in the graph)",
+                     "kernel": "lifetime_split_kernel + lifetime_finish_kernel + lifetime_retrace_kernel (per pass, "
+                               "in the graph)",
                      "work": "algorithmic FP64-op count of the reference's TraceOrbit (flop_model) over the "
                              "graph replay, divided by the replay's device time (the lifetime kernels are "
                              "~98% of it); traffic is per average pass",

@@ -137,6 +137,7 @@ CUDA_API = {
     "es_batch_collect": (_i32, [_vp, _vp, _vp]),
     "es_batch_stream": (_vp, [_vp]),
     "es_batch_launch_count": (_i64, [_vp]),
+    "es_batch_graph_kernels": (_i64, [_vp]),
     "es_batch_total_orbits": (_i64, [_vp]),
     "es_dgrid_create_seeded": (_i32, [_i32, _u32, _d, _d, _d, _d, _i32, _i64, C.POINTER(_vp)]),
     "es_dgrid_destroy": (_i32, [_vp]),

@@ -172,6 +172,10 @@ class BatchSweep:
     def launch_count(self) -> int:
         return int(N.cuda_lib().es_batch_launch_count(self._b))
 
+    def graph_kernels(self) -> int:
+        """Kernels one replay of the recorded graph launches."""
+        return int(N.cuda_lib().es_batch_graph_kernels(self._b))
+
 
 def finish_results(coherent: np.ndarray, incoherent: np.ndarray) -> dict:
     """SimulationRunner::FinishResults (src/SimulationRunner.cpp:153-198) on the

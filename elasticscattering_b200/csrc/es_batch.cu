@@ -497,6 +497,7 @@ struct es_batch {
 
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int64_t graph_kernels = 0;                 // kernel nodes of the recorded graph
     bool graph_dirty = true;
     bool has_instances = false;
 };
@@ -643,6 +644,8 @@ es_status ensure_pass_scratch(es_batch* b)
     return ES_OK;
 }
 
+int64_t count_kernel_nodes(cudaGraph_t g);
+
 // ES_BATCH_PASS_KERNELS: each pass in turn through the single-pass path's
 // kernels -- orbit table, lifetime walk and FP64 re-trace (split), or the FP64
 // lifetime kernel, then stages (b)+(c) for the pass's distinct relaxation
@@ -749,6 +752,7 @@ es_status capture(es_batch* b)
     }
     if (e_end != cudaSuccess) return bcuda(b, e_end, "batch graph capture");
     b->graph = g;
+    b->graph_kernels = count_kernel_nodes(g);
     if (b->exec) {
         // Same node sequence as the last recording (same passes, mode and
         // precision): update the executable graph's parameters in place, which
@@ -765,6 +769,21 @@ es_status capture(es_batch* b)
     ES_BCUDA(cudaGraphInstantiate(&b->exec, b->graph, 0), "batch graph instantiation");
     b->graph_dirty = false;
     return ES_OK;
+}
+
+// Kernel nodes of a recorded graph: the kernels one replay launches.
+int64_t count_kernel_nodes(cudaGraph_t g)
+{
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n == 0 || cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+    int64_t k = 0;
+    for (size_t i = 0; i < n; i++) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
 }
 
 es_status bind_batch(es_batch* b)
@@ -1312,6 +1331,8 @@ es_status es_batch_run(es_batch* b, double* out_sigma, es_metrics* out_metrics)
 void* es_batch_stream(es_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 int64_t es_batch_launch_count(const es_batch* b) { return b ? b->launches : 0; }
+
+int64_t es_batch_graph_kernels(const es_batch* b) { return b ? b->graph_kernels : 0; }
 
 int64_t es_batch_total_orbits(const es_batch* b) { return b ? b->total_orbits : 0; }
 

@@ -55,15 +55,14 @@ inline double integrand_factor(double particle_speed, int positions_per_row, dou
     return std::pow(1.0 / (3.0 * (positions_per_row - 1)), 2) * phi_integrand_factor * outside * 1e-8;
 }
 
-// Upper bound on the cell steps of one orbit: a full circle crosses at most
-// 4 * ceil(2 pi r / cell) + a few cell edges. Exceeding it is reported.
-// Whether a grid's walks are long enough for the split lifetime kernel's
-// warp-synced winner recompute: the straight-line mean free path through its
-// disks, L / (disks filed per cell x 2 r_i), at least half a cell. Around one
-// cell or more (5e15 m^-2, r_i 2 nm, 49 nm cells: 0.87) walks end after
-// differing numbers of cell steps and the synced form pays (3% per pass on
-// B200); well below (1e16 m^-2, r_i 5 nm, 35 nm cells: ~0.2) nearly every walk
-// ends in its first cell and it measured 30% slower.
+// Whether a grid's walks are long enough for the split lifetime kernel to
+// leave the winners' FP64 times to its finish kernel: the straight-line mean
+// free path through its disks, L / (disks filed per cell x 2 r_i), at least
+// half a cell. Around one cell or more (5e15 m^-2, r_i 2 nm, 49 nm cells:
+// 0.87) walks end after differing numbers of cell steps and the split finish
+// pays (5% per pass on B200); well below (1e16 m^-2, r_i 5 nm, 35 nm cells:
+// ~0.2) nearly every walk ends in its first cell and it measured 9-10%
+// slower than the finish inside the walk.
 inline bool long_walks(int64_t n_indexed, int cells_per_row, double cell_size, double impurity_radius)
 {
     const double cells = (double)cells_per_row * (double)cells_per_row;
@@ -72,6 +71,8 @@ inline bool long_walks(int64_t n_indexed, int cells_per_row, double cell_size, d
     return cell_size / (per_cell * 2.0 * impurity_radius) >= 0.5;
 }
 
+// Upper bound on the cell steps of one orbit: a full circle crosses at most
+// 4 * ceil(2 pi r / cell) + a few cell edges. Exceeding it is reported.
 inline int walk_cap_for(double radius, double cell)
 {
     const double steps = 4.0 * std::ceil(kPI2 * radius / cell) + 16.0;

@@ -353,7 +353,7 @@ __device__ __forceinline__ double finish_hit(const F& f, const OrbitD& o, int wi
 // metrics), or kSplitRetrace when the orbit must be re-traced in FP64. With
 // kDefer it returns kSplitHit instead of computing the winner's FP64 time: the
 // winning disk in win.x, a near-equal second in win.y (else -1), for
-// finish_hit.
+// finish_hit in lifetime_finish_kernel.
 template <class F, bool kDefer = false>
 __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos, SplitCounters& cnt, int& flags,
                                            double& out, int2& win, StartScan start = StartScan{-1, false})

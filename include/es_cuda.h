@@ -367,6 +367,9 @@ es_status es_batch_collect(es_batch* b, double* out_sigma, es_metrics* out_metri
 void* es_batch_stream(es_batch* b);
 /* Kernel launches issued by this batch (one per graph replay, one per grid copy). */
 int64_t es_batch_launch_count(const es_batch* b);
+/* Kernel nodes of the batch's recorded graph: the kernels one replay launches
+ * (0 before the first run). */
+int64_t es_batch_graph_kernels(const es_batch* b);
 /* Orbits per run of the current instance table. */
 int64_t es_batch_total_orbits(const es_batch* b);
 

@@ -286,3 +286,32 @@ def test_split_exact_batch_equals_fp64_batch(sweep_inputs, cuda_device):
     with BatchSweep(cuda_device, precision=N.ES_PRECISION_SPLIT, mode=N.ES_BATCH_PASS_KERNELS) as b:
         with pytest.raises(N.EsError):
             b.set_tuning(precision=N.ES_PRECISION_SPLIT_EXACT, mode=N.ES_BATCH_PERSISTENT)
+
+
+def _long_walks(grid) -> bool:
+    """The library's choice of the split-finish form for a pass on `grid`: the
+    grid's straight-line mean free path through its disks, in cells, >= 0.5."""
+    s = grid.GetSettings()
+    per_cell = grid.GetTotalImpurityCount() / float(s.cells_per_row ** 2)
+    return per_cell <= 0.0 or s.cell_size / (per_cell * 2.0 * s.impurity_radius) >= 0.5
+
+
+def test_graph_kernel_count(sweep_inputs, cuda_device):
+    """es_batch_graph_kernels counts the recorded graph's kernel nodes: per pass
+    the orbit table, the split walk, the winners' FP64 finish on long-walk
+    passes, the FP64 re-trace, integration and reduction (3 temperatures, one
+    group); two for the persistent mode (its kernel and the re-trace)."""
+    ext, grids = sweep_inputs
+    b, ids = new_batch(grids, cuda_device, N.ES_PRECISION_SPLIT, mode=N.ES_BATCH_PASS_KERNELS)
+    try:
+        assert b.graph_kernels() == 0
+        passes = make_passes(ext, grids, ids, fields=(1.5, 7.0))
+        b.set_passes(passes)
+        b.run()
+        long_by_grid = {ids[k]: _long_walks(grids[k]) for k in grids}
+        assert b.graph_kernels() == sum(6 if long_by_grid[p.grid] else 5 for p in passes)
+        b.set_tuning(mode=N.ES_BATCH_PERSISTENT)
+        b.run()
+        assert b.graph_kernels() == 2
+    finally:
+        b.close()
