@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(256, 5) lifetime_finish_kernel(LifetimeLaunch 
             dv2 pos;
             const OrbitD o = make_orbit(f, g, pos);
             int flags;
-            const double lt = finish_hit(f, o, win.x, win.y, flags);
+            const double lt = finish_hit<FinishFields, true>(f, o, win.x, win.y, flags);
             if (lt != lt) {
                 P.out[g] = 0.0;
                 const unsigned long long slot = atomicAdd(P.retrace_count, 1ull);

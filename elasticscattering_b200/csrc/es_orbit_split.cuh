@@ -250,6 +250,39 @@ __device__ __noinline__ double first_cross_angle_call(double cx, double cy, doub
     return first_cross_angle_open(o, dv2{ipx, ipy}, ir);
 }
 
+// first_cross_angle_open for lifetime_finish_kernel, with one GetAngle
+// instead of two where that gives the same bits. p1 lies at the centre angle
+// theta_u - beta of the disk direction theta_u and p2 at theta_u + beta
+// (beta = atan2(ys, xs)). Travelling counter-clockwise the orbit reaches p1
+// first, clockwise p2, unless the start angle lies between them. When that
+// point's travel angle plus the arc 2 beta stays 1e-5 rad clear of 2 pi, and
+// the arc is longer than 1e-5 rad, the other point's travel angle is the larger
+// (FP32 arc, error below 1e-6 rad), so the minimum is this one. Otherwise both
+// are computed as in first_cross_angle_open. A NaN first point returns NaN. A
+// NaN second point, past the shortcut's test, is one the reference drops
+// (AngleInRange is false), leaving the first.
+__device__ __forceinline__ double first_cross_angle_first(const OrbitD& o, dv2 ip, double ir)
+{
+    const double qx = o.center.x - ip.x;
+    const double qy = o.center.y - ip.y;
+    const double dist_sq = qx * qx + qy * qy;
+    const double dist = sqrt(dist_sq);
+    const double xs = (dist_sq + o.radius_sq - ir * ir) / (2.0 * dist);
+    const double ys = sqrt(o.radius_sq - xs * xs);
+    const double ux = (ip.x - o.center.x) / dist;
+    const double uy = (ip.y - o.center.y) / dist;
+    const dv2 p1 = {o.center.x + ux * xs + uy * ys, o.center.y + uy * xs + -ux * ys};
+    const dv2 p2 = {o.center.x + ux * xs + -uy * ys, o.center.y + uy * xs + ux * ys};
+    const double af = cross_angle(o.particle_angle, get_angle(o.clockwise ? p2 : p1, o), o.clockwise);
+    if (af != af) return af;
+    const float arc = 2.0f * fast_atan2((float)ys, (float)xs);
+    if (arc > 1e-5f && (float)af + arc < kTwoPiF - 1e-5f) return af;
+    const double as = cross_angle(o.particle_angle, get_angle(o.clockwise ? p1 : p2, o), o.clockwise);
+    if (as != as) return as;
+    const double a1 = o.clockwise ? as : af, a2 = o.clockwise ? af : as;  // the angles of p1, p2
+    return (a1 < a2) ? a1 : a2;
+}
+
 template <class F>
 __device__ __forceinline__ double first_cross_angle(const OrbitD& o, dv2 ip, double ir)
 {
@@ -330,15 +363,18 @@ __device__ __forceinline__ StartScan start_scan_shared(const F& f, dv2 pos, int 
 // the FP64 time of the crossing is still to be computed (finish_hit).
 enum SplitOutcome : int { kSplitDone = 0, kSplitRetrace = 1, kSplitHit = 2 };
 
-// The winning disk's reference time (FP64) and the bound clamp.
-template <class F>
+// The winning disk's reference time (FP64) and the bound clamp. kFirstPoint:
+// the crossing angles by first_cross_angle_first (lifetime_finish_kernel).
+template <class F, bool kFirstPoint = false>
 __device__ __forceinline__ double finish_hit(const F& f, const OrbitD& o, int win_k, int alt_k, int& flags)
 {
-    const double2 q = __ldg(f.imps() + win_k);
-    double t = first_cross_angle<F>(o, dv2{q.x, q.y}, f.imp_radius()) / f.w();
+    auto angle = [&](double2 q) {
+        return kFirstPoint ? first_cross_angle_first(o, dv2{q.x, q.y}, f.imp_radius())
+                           : first_cross_angle<F>(o, dv2{q.x, q.y}, f.imp_radius());
+    };
+    double t = angle(__ldg(f.imps() + win_k)) / f.w();
     if (alt_k >= 0) {
-        const double2 a = __ldg(f.imps() + alt_k);
-        const double t2 = first_cross_angle<F>(o, dv2{a.x, a.y}, f.imp_radius()) / f.w();
+        const double t2 = angle(__ldg(f.imps() + alt_k)) / f.w();
         t = (t < t2) ? t : t2;
     }
     flags = kTraceOk;
