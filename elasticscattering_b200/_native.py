@@ -159,6 +159,7 @@ CUDA_API = {
     "es_mlp_launch_count": (_i64, [_vp]),
     "es_mlp_stream": (_vp, [_vp]),
     "es_debug_trace": (_i32, [_vp, _d, _d, _i32, _i32, _d, _d, _d, _d, _d, _i32, _i32, C.POINTER(_d)]),
+    "es_debug_finish_retrace": (_i32, [_vp, _i32]),
     "es_debug_next_cell": (_i32, [_vp, _d, _d, _d, _i32, _d, C.POINTER(ImpuritySettings), _vp, _vp,
                                   C.POINTER(_i32)]),
 }

@@ -75,6 +75,7 @@ struct es_ctx {
     unsigned long long* d_retrace_count = nullptr;
     long long retrace_cap = 0;
     es_tuning tuning{es::kLifetimePerThreadDefer};
+    int finish_retrace_every = 0;  // es_debug_finish_retrace
     bool lifetimes_valid = false;
     int row0 = 0, row1 = 0;  // start rows [row0, row1) of the passes (es_set_rows); row1 = dim by default
 };
@@ -166,6 +167,7 @@ es::LifetimeLaunch make_launch(const es_ctx* ctx, double magnetic_field, double 
     L.retrace_count = ctx->d_retrace_count;
     L.retrace_cap = ctx->retrace_cap;
     L.orbit_table = ctx->d_orbit_table;
+    L.finish_retrace_every = ctx->finish_retrace_every;
     es::host::split_constants(L);
     return L;
 }
@@ -804,6 +806,15 @@ es_status es_debug_trace(es_ctx* ctx, double px, double py, int32_t q, int32_t p
     cudaFree(d);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "es_debug_trace");
     if (*out_lifetime < 0.0) return fail(ctx, ES_ERR_BAD_ARG, "es_debug_trace: position outside the impurity grid");
+    return ES_OK;
+}
+
+es_status es_debug_finish_retrace(es_ctx* ctx, int32_t every)
+{
+    if (!ctx) return ES_ERR_BAD_ARG;
+    if (every < 0) return fail(ctx, ES_ERR_BAD_ARG, "es_debug_finish_retrace: every must be >= 0 (got %d)", every);
+    ctx->finish_retrace_every = every;
+    ctx->lifetimes_valid = false;
     return ES_OK;
 }
 

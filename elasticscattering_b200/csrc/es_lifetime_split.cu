@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(256, 5) lifetime_finish_kernel(LifetimeLaunch 
             const OrbitD o = make_orbit(f, g, pos);
             int flags;
             const double lt = finish_hit<FinishFields, true>(f, o, win.x, win.y, flags);
-            if (lt != lt) {
+            if (lt != lt || (P.finish_retrace_every > 0 && g % P.finish_retrace_every == 0)) {
                 P.out[g] = 0.0;
                 const unsigned long long slot = atomicAdd(P.retrace_count, 1ull);
                 if (slot < (unsigned long long)P.retrace_cap) P.retrace[slot] = g | kRetraceFromFinish;

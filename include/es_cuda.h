@@ -224,6 +224,14 @@ void* es_stream(es_ctx* ctx);
 /* Number of kernel launches this context has issued since creation. */
 int64_t es_launch_count(const es_ctx* ctx);
 
+/* Test hook for the split path's finish kernel: on passes that leave their
+ * winners to it (long walks), the hit of every orbit whose index is a multiple
+ * of `every` goes to the FP64 re-trace as a winner whose crossing point the
+ * reference drops would, and the re-trace subtracts the walk's counters. The
+ * lifetimes and every counter but `retraced_fp64` must stay as without it.
+ * 0 (the default) turns it off. No reference counterpart. */
+es_status es_debug_finish_retrace(es_ctx* ctx, int32_t every);
+
 /* Known-answer hook for the device geometry: one GetNextCell step
  * (src/sim/es/cell_grid.h:132-181) evaluated by the FP64 device code on one
  * thread. in6/out6 = (pos.x, pos.y, incident_angle, dphi, cell.x, cell.y).

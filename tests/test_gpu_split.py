@@ -196,3 +196,32 @@ def test_split_exact_sigma_equals_fp64(cuda_device):
                 for a, b in zip(ip, ie):
                     assert np.array_equal(a.particle_lifetimes, b.particle_lifetimes)
                     assert np.array_equal(a.xx_buffer, b.xx_buffer) and np.array_equal(a.xy_buffer, b.xy_buffer)
+
+
+@pytest.mark.parametrize("every", [5, 13])  # the re-trace list holds a quarter of the pass
+def test_finish_retrace_keeps_lifetimes_and_counters(cuda_device, every):
+    """The finish kernel hands a winner whose crossing point the reference drops
+    (NaN) to the FP64 re-trace, which subtracts the walk's counters of that orbit
+    before adding its own. es_debug_finish_retrace forces that path for the hit
+    of every `every`-th orbit on a long-walk (config-1) grid: the lifetimes must
+    stay bit-identical and every counter but retraced_fp64 unchanged, with more
+    orbits re-traced."""
+    w = workloads.config1()
+    g = Grid.from_seed(w.seed(0), w.region_size, w.region_extends, w.density, w.impurity_radius,
+                       w.target_cell_population)
+    lib = N.cuda_lib()
+    with SimulationCUDA(65, 33, g.info(), device=cuda_device, precision=N.ES_PRECISION_SPLIT) as sim:
+        assert lib.es_debug_finish_retrace(sim.ctx, -1) == N.ES_ERR_BAD_ARG
+        for coherent in (True, False):
+            sim.InitSample(g, settings_of(w), coherent)
+            for B in (1.0, 20.0):
+                N.check(lib.es_debug_finish_retrace(sim.ctx, 0), sim.ctx)
+                ref, mref = sim.ComputeLifetimes(B)
+                N.check(lib.es_debug_finish_retrace(sim.ctx, every), sim.ctx)
+                got, mgot = sim.ComputeLifetimes(B)
+                assert np.array_equal(ref.view(np.int64), got.view(np.int64)), (coherent, B)
+                for k in mref:
+                    if k != "retraced_fp64":
+                        assert mgot[k] == mref[k], (coherent, B, k, mgot[k], mref[k])
+                assert mgot["retraced_fp64"] > mref["retraced_fp64"]
+        N.check(lib.es_debug_finish_retrace(sim.ctx, 0), sim.ctx)
