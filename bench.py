@@ -13,8 +13,8 @@ three average samples), all 32 fields and 3 temperatures: 192 sector passes,
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload config2|config1|...]
 
 The line also carries: the same passes in FP64 (the split path's error per
-result), the plain per-pass FP64 GPU path on the same passes (the north star's
-20x bar), stages (b)+(c) against HBM, the full 64-sample sweep timed once, the
+result), the plain per-pass FP64 GPU path on the same passes (the stated
+20x bar for the batched split path), stages (b)+(c) against HBM, the full 64-sample sweep timed once, the
 config-1 sweep (257^2 x 516 orbits, 5 fields), the public API end to end, and
 the reference's own CPU code on a bounded sample of the slice.
 
@@ -648,7 +648,7 @@ def run_batched(args) -> None:
     (default: one sample of each start grid, all 32 fields, T in {0, 10, 40} K,
     both sectors: 192 passes, 11.4 G orbits). Reports, besides the split path's
     throughput: the FP64 batch of the same passes (the per-result error), the
-    plain per-pass FP64 GPU path on the same work (the north star's 20x bar),
+    plain per-pass FP64 GPU path on the same work (the stated 20x bar),
     stages (b)+(c) against HBM, the full 64-sample sweep timed once (split over
     the GPUs by LPT on estimated cost), the config-1 sweep, and the reference
     CPU code on a bounded sample of the slice."""
@@ -967,7 +967,7 @@ def run_batched(args) -> None:
                             "speedup_same_work": plain_s / (step_ms * 1e-3),
                             "max_rel_vs_plain_fp64": worst_vs_plain,
                             "note": "the same passes through es_compute_sigmas (blocking, FP64 contexts), "
-                                    "against the timed split graph replay; north-star bar 20x"},
+                                    "against the timed split graph replay; the stated bar is 20x"},
         "full_sweep": full_sweep,
         "config1_sweep": c1,
         "host_grid_build_s": grid_build_s,
@@ -1017,18 +1017,18 @@ def run_surrogate(args) -> None:
     train_s_time = time.perf_counter() - t0
     # fallback threshold: calibrated on held-out simulator answers so that the
     # network's own answers meet the 1% bar at the 95th percentile
-    cal_q = sim.snapped(S.sample_queries(args.judge_queries * 2, seed=50))
+    cal_q = sim.snapped(S.sample_queries(args.eval_queries * 2, seed=50))
     tol = sur.calibrate(cal_q, sim(cal_q), target=0.01, quantile=0.95)
 
     Q = 4096
     batches = [sim.snapped(S.sample_queries(Q, seed=100 + k)) for k in range(args.steps + args.warmup)]
-    # the simulator on the same kind of batch: latency and the error judge
-    judge_q = batches[-1][:args.judge_queries]
+    # the simulator on the same kind of batch: latency and the error reference
+    eval_q = batches[-1][:args.eval_queries]
     t0 = time.perf_counter()
-    truth = sim(judge_q)
+    truth = sim(eval_q)
     sim_s = time.perf_counter() - t0
-    sim_ms_per_query = 1e3 * sim_s / len(judge_q)
-    nn_only = (np.abs(S.untarget(judge_q, ens.predict(S.features(judge_q))[0]).mean(axis=0) - truth)
+    sim_ms_per_query = 1e3 * sim_s / len(eval_q)
+    nn_only = (np.abs(S.untarget(eval_q, ens.predict(S.features(eval_q))[0]).mean(axis=0) - truth)
                / np.abs(truth)).max(axis=1)
 
     def serve(tolerance: float) -> dict:
@@ -1042,7 +1042,7 @@ def run_surrogate(args) -> None:
             t_total += time.perf_counter() - t0
             net_ms.append(1e3 * tm["network_s"])
             fb_frac.append(float(fb.mean()))
-        sig, fb, _, _ = sur.query(judge_q)
+        sig, fb, _, _ = sur.query(eval_q)
         err = (np.abs(sig - truth) / np.abs(truth)).max(axis=1)
         ans = ~fb
         med_fb = statistics.median(fb_frac)
@@ -1066,13 +1066,13 @@ def run_surrogate(args) -> None:
     sur.tolerance = 0.01
     one_nn, one_sim = [], []
     for k in range(3):
-        sur.query(judge_q[k:k + 1])
+        sur.query(eval_q[k:k + 1])
     for k in range(64):
-        one_nn.append(1e3 * sur.query(judge_q[k:k + 1])[3]["network_s"])
-    sim(judge_q[:1])
+        one_nn.append(1e3 * sur.query(eval_q[k:k + 1])[3]["network_s"])
+    sim(eval_q[:1])
     for k in range(8):
         t0 = time.perf_counter()
-        sim(judge_q[k:k + 1])
+        sim(eval_q[k:k + 1])
         one_sim.append(1e3 * (time.perf_counter() - t0))
     single = {"network_ms_median": statistics.median(one_nn), "simulator_ms_median": statistics.median(one_sim),
               "latency_gain_median": statistics.median(one_sim) / statistics.median(one_nn),
@@ -1094,7 +1094,7 @@ def run_surrogate(args) -> None:
         "single_query_latency": single,
         "simulator_latency_ms_per_query": sim_ms_per_query,
         "simulator_latency_ms_per_batch_extrapolated": sim_ms_per_query * Q,
-        "network_only_error": {"queries": int(len(judge_q)), "p50": float(np.median(nn_only)),
+        "network_only_error": {"queries": int(len(eval_q)), "p50": float(np.median(nn_only)),
                                "p95": float(np.quantile(nn_only, 0.95)), "max": float(nn_only.max())},
         "training": {"grid_build_s": build_s, "data_s": data_s, "train_s": train_s_time,
                      "final_loss": losses[-1]},
@@ -1191,7 +1191,7 @@ def main() -> None:
     ap.add_argument("--workload", default="config2", choices=sorted(workloads.WORKLOADS) + ["config2", "config4"])
     ap.add_argument("--train-points", type=int, default=20000, help="config4: simulator runs for training")
     ap.add_argument("--train-steps", type=int, default=36000, help="config4: Adam steps")
-    ap.add_argument("--judge-queries", type=int, default=512, help="config4: queries checked against the simulator")
+    ap.add_argument("--eval-queries", type=int, default=512, help="config4: queries checked against the simulator")
     ap.add_argument("--ref-rows", type=int, default=2, help="start-position rows per CPU process")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--samples", type=int, default=0,

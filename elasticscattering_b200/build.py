@@ -129,7 +129,7 @@ def build_host(force: bool = False) -> list[Path]:
 
 
 def build_oracle() -> None:
-    """Test checkers: oracle/liboracle.so, and oracle/_ref when the reference tree exists."""
+    """Test oracles: oracle/liboracle.so, and oracle/_ref when the reference tree exists."""
     _run(["make", "-s", "-C", str(ROOT / "oracle")])
 
 

@@ -26,7 +26,7 @@
 //
 // Split-precision contexts (fp32 = 1) evaluate GetSigma in FP32 (es_sigma32.cuh:
 // cancellation-free form, angles formed and reduced in FP64) and keep every
-// sum in FP64, as the north-star split asks of the Simpson integrals; the
+// sum in FP64: the Simpson integrals in FP32 with FP64 accumulation; the
 // plain path keeps the reference's FP64 expression operation by operation.
 #include "es_internal.h"
 #include "es_sigma32.cuh"

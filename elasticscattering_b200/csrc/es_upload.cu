@@ -16,7 +16,7 @@ namespace es {
 
 namespace {
 
-constexpr size_t kDirectBelow = size_t(1) << 20;  // smaller copies take the driver's path
+constexpr size_t kDirectBelow = size_t(1) << 20;  // smaller copies take the CUDA driver's own staging
 constexpr int kMaxThreads = 8;
 constexpr size_t kStripeMin = size_t(1) << 20;     // bytes per memcpy thread, at least
 

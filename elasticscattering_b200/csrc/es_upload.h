@@ -1,13 +1,13 @@
 // es_upload.h - host-to-device copies of caller arrays held in pageable memory,
 // through a pinned staging ring.
 //
-// A cudaMemcpyAsync from pageable memory is staged by the driver through its
+// A cudaMemcpyAsync from pageable memory is staged by the CUDA driver through its
 // own pinned buffers on the calling thread. The grid uploads of the C ABI
 // (es_upload_grid, es_batch_add_grid: tens to hundreds of MB per grid) instead
 // copy each chunk into a pinned ring slot with several host threads while the
 // DMA of the previous chunk runs. A source that is already pinned (or
 // registered, managed, device) memory is copied directly, and small copies
-// take the driver's path. The reference uploads with clEnqueueWriteBuffer from
+// take the CUDA driver's own staging. The reference uploads with clEnqueueWriteBuffer from
 // its std::vectors (src/sim/SimulationCL.cpp:121-122).
 #pragma once
 

@@ -5,7 +5,7 @@
 // instead of the reference's print-and-exit; the CLI turns them into a
 // non-zero exit code.
 //
-// Keys this build adds (ignored by the reference): `precision
+// Keys this runtime adds (ignored by the reference): `precision
 // fp64|split|split_exact` (default fp64: the reference's arithmetic;
 // split_exact: the split walk with FP64 integration, the same sigma as fp64),
 // `batched 0|1` (1: every sample,

@@ -2,7 +2,7 @@
 //
 // The reference files each impurity into up to 9 per-cell std::vectors
 // (std::set-deduplicated probes, then corner checks) and concatenates them
-// row-major. This build computes the same cells per impurity and places the
+// row-major. This runtime computes the same cells per impurity and places the
 // impurities with a two-pass stable counting sort, which yields the identical
 // ordered array and cumulative index without per-cell containers.
 #include "grid.h"

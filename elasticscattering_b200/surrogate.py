@@ -6,7 +6,7 @@ trained on the GPU by the library's own forward and backward kernels) answers
 sigma queries; wherever the members disagree by more than the tolerance (their
 standard deviation over |mean|, per output), the query is answered by the
 simulator instead -- the batched split-precision path, which also generates the
-training data and judges the surrogate's error.
+training data and measures the surrogate's error.
 
 Features (each mapped onto about [-1, 1]): log B, T, log density, impurity
 radius, log tau. Targets: the total sigma (coherent + incoherent sector, as the

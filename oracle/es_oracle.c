@@ -1,7 +1,7 @@
 /* es_oracle.c - CPU restatement of ElasticScattering's FP64 real-space
  * conductivity path (impurity grid, orbit lifetimes, Simpson integration).
  *
- * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path. Loaded by tests/,
+ * TEST INFRASTRUCTURE ONLY: the oracle for the CUDA path. Loaded by tests/,
  * __graft_entry__.smoke() and bench.py's cpu_baseline leg; never by the product.
  *
  * Every function restates the reference operation by operation (same operand

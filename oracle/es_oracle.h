@@ -1,7 +1,7 @@
 /* es_oracle.h - CPU restatement of ElasticScattering's FP64 real-space
  * conductivity path.
  *
- * TEST INFRASTRUCTURE ONLY. The oracle is the checker for the CUDA path: only
+ * TEST INFRASTRUCTURE ONLY. The oracle verifies the CUDA path: only
  * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load it. The
  * product (libes_cuda.so, the host runtime) never links or calls it.
  *

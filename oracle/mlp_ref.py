@@ -1,6 +1,6 @@
 """CPU FP64 restatement of the surrogate network (test infrastructure only).
 
-The checker for the GPU training kernels of elasticscattering_b200/csrc/es_mlp.cu:
+The oracle for the GPU training kernels of elasticscattering_b200/csrc/es_mlp.cu:
 the same network (5 -> 256 x 4 -> 2, GELU, one member) evaluated in FP64, with
 values rounded to BF16 exactly where the GPU path stores BF16 (inputs, hidden
 weights, hidden activations that feed the next hidden layer, back-propagated

@@ -2,7 +2,7 @@
  *
  * TEST INFRASTRUCTURE ONLY: used when compiling the reference's own CPU
  * sources (src/sim/Grid.cpp, src/sim/SimulationCPU.cpp) on Linux so that the
- * reference can serve as the checker of the oracle restatement and as the timed
+ * reference can verify the oracle restatement and serve as the timed
  * CPU baseline. Nothing in the product links this.
  *
  * The reference uses LARGE_INTEGER / QueryPerformanceCounter /

@@ -22,7 +22,7 @@ SimulationCL::SimulationCL(int p_particles_per_row, int p_values_per_quadrant, c
     : Simulation(p_particles_per_row, p_values_per_quadrant, grid_info)
 {
     (void)p_print_info;
-    std::cout << "The OpenCL backend is not part of this build." << std::endl;
+    std::cout << "The OpenCL backend is not compiled into this harness." << std::endl;
     exit(0);
 }
 

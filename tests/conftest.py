@@ -16,7 +16,7 @@ ROOT = Path(__file__).resolve().parent.parent
 GOLDEN = ROOT / "tests" / "golden"
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
-sys.path.insert(0, str(ROOT / "oracle"))  # mlp_ref: the surrogate network's FP64 checker
+sys.path.insert(0, str(ROOT / "oracle"))  # mlp_ref: the surrogate network's FP64 oracle
 
 
 def pytest_configure(config):
@@ -45,7 +45,7 @@ def golden():
 @pytest.fixture(scope="session")
 def cuda_device():
     """Every GPU test goes through here: no device means a hard failure when the
-    test was explicitly selected with -m gpu on a GPU box, a skip otherwise."""
+    test was explicitly selected with -m gpu on a GPU machine, a skip otherwise."""
     if not gpu_available():
         pytest.skip("no CUDA device")
     from elasticscattering_b200 import _native

@@ -1,4 +1,4 @@
-"""ctypes access to the CPU checkers (test infrastructure only).
+"""ctypes access to the CPU oracles (test infrastructure only).
 
 - liboracle.so : the C restatement of the reference's FP64 path (oracle/es_oracle.c)
 - libes_ref.so : the reference's own CPU sources compiled in place (oracle/_ref)

@@ -1,6 +1,6 @@
 """The reference's own CPU build (oracle/_ref/libes_ref.so) run over many processes.
 
-TEST INFRASTRUCTURE ONLY (the checker of the full-size parity tests). The
+TEST INFRASTRUCTURE ONLY (the oracle of the full-size parity tests). The
 reference is single-threaded (src/sim/SimulationCPU.cpp:112-135); a full
 config-1 sector pass takes ~30 s on one core. Here the start-position rows of
 each pass are split into disjoint ranges, each range runs the body of the

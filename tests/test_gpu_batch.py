@@ -2,7 +2,7 @@
 
 Each batched pass must reproduce what one Simulation::ComputeSigmas call
 returns for it (src/sim/Simulation.h:128): the per-pass FP64 path
-(SimulationCUDA, ES_PRECISION_FP64) is the judge. Bars:
+(SimulationCUDA, ES_PRECISION_FP64) is the reference. Bars:
 - ES_PRECISION_FP64 batch: sigma within 1e-9 relative -- the plain path's parity
   bar; only the summation order and the fixed-point rounding of the work-item
   sums differ (observed ~1e-11 on sigma_xy, whose terms cancel) -- and identical

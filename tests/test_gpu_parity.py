@@ -1,6 +1,6 @@
 """Parity of the CUDA path (libes_cuda.so, called through its C ABI) with the oracle.
 
-Bars (north star): the same hit/no-hit decision for every orbit, and sigma within
+Bars (the parity target): the same hit/no-hit decision for every orbit, and sigma within
 1e-9 relative of the reference's FP64 results on the same seeded inputs.
 Per-orbit lifetimes are additionally held to 1e-9 relative (they differ from the
 CPU only through the last bits of asin; the phase constants are tabulated with
@@ -19,7 +19,7 @@ from elasticscattering_b200 import _native as N
 
 pytestmark = pytest.mark.gpu
 
-SIGMA_RTOL = 1e-9      # north-star sigma tolerance, relative
+SIGMA_RTOL = 1e-9      # plain-path sigma tolerance, relative
 LIFETIME_RTOL = 1e-9   # per-orbit lifetime tolerance, relative
 E = 1.60217646e-19
 M = 5.0 * 9.10938188e-31

@@ -11,7 +11,7 @@ same seeded inputs, at their full sizes:
 - 1025^2 x 1028 orbits, 1e16 m^-2, r_i 5 nm, B = 40 T: three bands of 16 start
   rows of the full-size pass, and sigma at 129^2 start positions.
 
-Bars (north star): the same hit/no-hit decision for every orbit (no class flip:
+Bars (the parity target): the same hit/no-hit decision for every orbit (no class flip:
 no lifetime, hit, clamped to the sector bound), sigma within 1e-9 relative on the
 plain FP64 path and within 1e-6 on the FP32/FP64 split path, and the
 reference's metric counters equal. Per-orbit lifetimes are held to 1e-6

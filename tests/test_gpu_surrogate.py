@@ -1,9 +1,9 @@
-"""The learned surrogate's GPU kernels (es_mlp_*) against the FP64 checker, and
+"""The learned surrogate's GPU kernels (es_mlp_*) against the FP64 oracle, and
 the surrogate with fallback against the simulator it stands in for.
 
 - forward pass of every ensemble member vs oracle/mlp_ref.py (same BF16
   roundings, FP64 elsewhere): within 2e-3 relative (norm);
-- loss and every parameter gradient vs the checker: loss within 1e-3, each
+- loss and every parameter gradient vs the oracle: loss within 1e-3, each
   weight and bias gradient within 2e-2 relative (norm) -- the residue is the
   GPU's FP32 accumulation and GELU, and the BF16 roundings they occasionally flip;
   the 256 x 256 layers' gradients come from the tcgen05 kernel;
@@ -48,7 +48,7 @@ def randomized_params(seed: int) -> np.ndarray:
     return p
 
 
-def test_forward_matches_fp64_checker(cuda_device):
+def test_forward_matches_fp64_oracle(cuda_device):
     p = randomized_params(11)
     x = np.random.default_rng(2).uniform(-1, 1, size=(300, 5)).astype(np.float32)
     with S.MLPEnsemble(4, cuda_device) as ens:
@@ -63,7 +63,7 @@ def test_forward_matches_fp64_checker(cuda_device):
 
 
 @pytest.mark.parametrize("rows", [200, 300, 600])
-def test_gradients_match_fp64_checker(cuda_device, rows):
+def test_gradients_match_fp64_oracle(cuda_device, rows):
     """The 256 x 256 layers' input and weight gradients run on the tensor cores
     (tcgen05): 200 rows leave the reduction of the weight gradient partly
     zero-filled; 300 and 600 take it over two and three steps of 256 rows."""
@@ -92,9 +92,9 @@ def test_device_query_matches_host_path(cuda_device, n):
     """es_mlp_query (features, every member, exp/sigma_0/Drude, mean and spread
     on the device) against the host path it replaces (features() ->
     es_mlp_predict -> untarget() -> numpy mean and spread) and the FP64
-    checker. n <= 256 runs the one-kernel CUDA-core path, whose hidden layers
+    oracle. n <= 256 runs the one-kernel CUDA-core path, whose hidden layers
     sum in another FP32 order than the tensor cores: its member outputs are
-    held to the checker's forward bar; n > 256 runs the batched tensor-core
+    held to the oracle's forward bar; n > 256 runs the batched tensor-core
     pass on device-made features and must equal the host path to rounding."""
     p = randomized_params(21)
     q = S.sample_queries(n, seed=5)

@@ -1,4 +1,4 @@
-"""Pins the oracle (oracle/es_oracle.c) before it is trusted as the GPU checker.
+"""Pins the oracle (oracle/es_oracle.c) before the GPU tests trust it.
 
 1. Known answers of the reference's unit tests (tests/es/*.h, tests/sim/SimpsonWeightsTest.h).
 2. The reference's golden sigma tables (tests/sim/SigmaIntegrationTest.h:84-138) at the

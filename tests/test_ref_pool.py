@@ -1,5 +1,5 @@
 """The multi-process runner of the reference's CPU build (tests/ref_pool.py),
-which the full-size GPU parity tests use as their checker, reproduces the
+which the full-size GPU parity tests use as their oracle, reproduces the
 reference's own single-process SimulationCPU bit for bit: lifetimes, metric
 counters and sigma, on config 0 and on a band of rows."""
 from __future__ import annotations

@@ -1,4 +1,4 @@
-"""Surrogate pieces that need no GPU: the FP64 network checker, features and
+"""Surrogate pieces that need no GPU: the FP64 network oracle, features and
 targets, the query draws and the C ABI's parameter count."""
 from __future__ import annotations
 
@@ -11,7 +11,7 @@ from elasticscattering_b200 import surrogate as S
 
 
 def test_reference_backprop_matches_finite_differences():
-    """The checker's analytic gradient (rounding off) against central differences."""
+    """The oracle's analytic gradient (rounding off) against central differences."""
     rng = np.random.default_rng(1)
     p = S.init_params(1, seed=3).astype(np.float64)
     x = rng.uniform(-1, 1, size=(6, 5))
