@@ -96,6 +96,10 @@ inline void split_constants(LifetimeLaunch& L)
     L.sc_band_d = 0.02f * L.sc_ir;
     L.sc_inv4r = 0.25f * L.sc_inv_r;
     L.sc_tangent_tol = (float)((0.01 * L.cell_size * L.cell_size) * (double)L.sc_inv_r + 2e-7 * L.cell_size);
+    // M = ceil(2^64 / d): for n, d < 2^32, (n M) >> 64 = floor(n / d), since
+    // n M / 2^64 exceeds n / d by less than 2^-32 < 1 / d
+    L.inv_phase = L.n_phase > 0 ? UINT64_MAX / (uint64_t)L.n_phase + 1 : 0;
+    L.inv_dim = L.dim > 0 ? UINT64_MAX / (uint64_t)L.dim + 1 : 0;
 }
 
 // Sector constants of Simulation::InitSample (src/sim/Simulation.h:111-126).

@@ -83,6 +83,10 @@ struct LifetimeLaunch {
     // es_host_math.h): as kernel parameters they are constant-bank operands
     // instead of registers.
     float sc_r, sc_inv_r, sc_ir, sc_lo2, sc_hi2, sc_eps2, sc_band_d, sc_inv4r, sc_tangent_tol;
+    // ceil(2^64 / n_phase) and ceil(2^64 / dim) (split_constants): the 32-bit
+    // quotients of an orbit index by them as one multiply-high each (exact for
+    // dividends and divisors below 2^32); 0: divide.
+    unsigned long long inv_phase, inv_dim;
     // Test hook (es_debug_finish_retrace): the finish kernel hands the hit of
     // every orbit whose index is a multiple of this to the FP64 re-trace, as it
     // does a NaN finish (0: none).

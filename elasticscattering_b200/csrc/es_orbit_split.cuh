@@ -84,6 +84,8 @@ struct LaunchFields {
     __device__ __forceinline__ float band_d() const { return P.sc_band_d; }
     __device__ __forceinline__ float inv4r() const { return P.sc_inv4r; }
     __device__ __forceinline__ float tangent_tol() const { return P.sc_tangent_tol; }
+    __device__ __forceinline__ unsigned long long inv_phase() const { return P.inv_phase; }
+    __device__ __forceinline__ unsigned long long inv_dim() const { return P.inv_dim; }
 };
 
 struct SharedFields {
@@ -123,6 +125,8 @@ struct SharedFields {
     __device__ __forceinline__ float band_d() const { return P->sc_band_d; }
     __device__ __forceinline__ float inv4r() const { return P->sc_inv4r; }
     __device__ __forceinline__ float tangent_tol() const { return P->sc_tangent_tol; }
+    __device__ __forceinline__ unsigned long long inv_phase() const { return P->inv_phase; }
+    __device__ __forceinline__ unsigned long long inv_dim() const { return P->inv_dim; }
 };
 
 __device__ __forceinline__ float wrap2pi(float a) { return a - kTwoPiF * floorf(a * (1.0f / kTwoPiF)); }
@@ -391,8 +395,8 @@ __device__ __forceinline__ double finish_hit(const F& f, const OrbitD& o, int wi
 // winning disk in win.x, a near-equal second in win.y (else -1), for
 // finish_hit in lifetime_finish_kernel.
 template <class F, bool kDefer = false>
-__device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos, SplitCounters& cnt, int& flags,
-                                           double& out, int2& win, StartScan start = StartScan{-1, false})
+__device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos, int cx, int cy, SplitCounters& cnt,
+                                           int& flags, double& out, int2& win, StartScan start = StartScan{-1, false})
 {
     const double r64 = o.radius;
     // The pass's FP32 constants (split_constants, es_host_math.h): r, 1/r, r_i;
@@ -412,8 +416,7 @@ __device__ __forceinline__ int trace_split(const F& f, const OrbitD& o, dv2 pos,
     const float dir = o.clockwise ? -1.0f : 1.0f;
     const float psi0 = (float)(o.clockwise ? o.particle_angle - kHALF_PI : o.particle_angle + kHALF_PI);
 
-    int cx = (int)((pos.x - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
-    int cy = (int)((pos.y - f.spawn_start()) / f.spawn_size() * (double)f.cpr());
+    // (cx, cy): the start cell, (int)((pos - start) / size * cpr) per axis, from the caller.
 
     // Start-cell InsideImpurity scan (lifetime.h:90-99), FP32 with an FP64 band,
     // unless the caller's lanes shared it (start_scan_shared).
@@ -753,12 +756,16 @@ __device__ __forceinline__ OrbitD make_orbit(const F& f, long long g, dv2& pos)
     int v, i, j;
     if (F::kOrbitTable && (unsigned long long)g < (1ull << 32)) {
         // 32-bit index arithmetic (every pass below 2^32 orbits): a 64-bit
-        // division by a run-time divisor is a long instruction sequence
+        // division by a run-time divisor is a long instruction sequence, a
+        // 32-bit one a shorter one, a multiply-high by ceil(2^64 / divisor)
+        // (split_constants) one instruction pair
         const unsigned g32 = (unsigned)g, np = (unsigned)f.n_phase(), d = (unsigned)f.dim();
-        const unsigned pidx = g32 / np;
+        const unsigned long long mp = f.inv_phase(), md = f.inv_dim();
+        const unsigned pidx = mp ? (unsigned)__umul64hi((unsigned long long)g32, mp) : g32 / np;
         v = (int)(g32 - pidx * np);
-        i = (int)(pidx % d);
-        j = (int)(pidx / d);
+        const unsigned row = md ? (unsigned)__umul64hi((unsigned long long)pidx, md) : pidx / d;
+        i = (int)(pidx - row * d);
+        j = (int)row;
     } else {
         v = (int)(g % f.n_phase());
         const long long pidx = g / f.n_phase();
@@ -829,7 +836,7 @@ __device__ __forceinline__ bool split_orbit(const F& f, long long g, SplitCounte
         return false;
     }
     int2 win;
-    if (trace_split(f, o, pos, cnt, flags, lt, win, start) == kSplitRetrace) {
+    if (trace_split(f, o, pos, cx, cy, cnt, flags, lt, win, start) == kSplitRetrace) {
         cnt = SplitCounters{0, 0, 0, 0};
         flags = kTraceOk;
         return true;
@@ -885,7 +892,7 @@ __device__ __forceinline__ int split_orbit_walk(const F& f, long long g, unsigne
         atomicOr(f.error(), kErrStartCell);
         return kSplitDone;
     }
-    const int st = trace_split<F, true>(f, o, pos, cnt, flags, lt, win, start);
+    const int st = trace_split<F, true>(f, o, pos, cx, cy, cnt, flags, lt, win, start);
     if (st == kSplitRetrace) {
         cnt = SplitCounters{0, 0, 0, 0};
         flags = kTraceOk;
