@@ -112,6 +112,26 @@ def test_grid_generation_properties():
         assert gd.GetCellsPerRow() == 2 and gd.GetTotalImpurityCount() == 7
 
 
+def test_grid_arrays_point_at_the_grid_itself():
+    """Grid.arrays(): the pointers es_upload_grid and es_batch_add_grid read in
+    place hold what GetImpurities / GetIndex copy out, and stay the same pointers
+    across calls (no copy is made)."""
+    import ctypes as C
+
+    g = Grid.from_seed(7, 1e-6, 3.8e-7, 5e15, 2e-9, 12)
+    xy, n, idx = g.arrays()
+    assert n == g.GetTotalImpurityCount() > 0
+    cells = g.GetCellsPerRow() ** 2
+    got_xy = np.ctypeslib.as_array(C.cast(xy, C.POINTER(C.c_double)), shape=(2 * n,))
+    got_idx = np.ctypeslib.as_array(C.cast(idx, C.POINTER(C.c_int32)), shape=(cells,))
+    assert np.array_equal(got_xy, g.GetImpurities().ravel())
+    assert np.array_equal(got_idx, g.GetIndex())
+    xy2, _, idx2 = g.arrays()
+    assert xy2.value == xy.value and idx2.value == idx.value
+    empty = Grid.from_list([], 1e-6, 0.0, 2e-9, 12)
+    assert empty.arrays()[:2] == (None, 0)
+
+
 def test_grid_config_errors_raise():
     with pytest.raises(EsError, match="Woah"):
         Grid.from_seed(1, 1e-5, 1e-5, 1e20, 2e-9, 10)
